@@ -1,0 +1,137 @@
+// common.cuh -- device-side data layout and exact-arithmetic helpers shared by every kernel.
+//
+// Layout (one handle = k scenes over packed index spaces):
+//   particles  : scene s owns packed ids [p_begin, p_end); state arrays are in id order,
+//                pos4 = (x, y, z, mass), vel4 = (u, v, w, type-as-int-bits);
+//   cells      : scene s owns packed cells [c_begin, c_begin + n^3); cell (i,j,k) of the
+//                scene is c_begin + (i*n + j)*n + k (z fastest, the reference's loop order);
+//   faces      : scene s owns [f_begin, f_begin + 3 n^2 (n+1)): x faces ((n+1),n,n), then
+//                y faces (n,(n+1),n), then z faces (n,n,(n+1)), each z fastest.
+// All float arithmetic is written in the reference's expression order; the library is built
+// with --fmad=false so no multiply-add is contracted, which keeps every stage bit-exact
+// against the CPU restatement on identical inputs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ariel.h"
+
+namespace ariel {
+
+constexpr int kMaxScenes = 1024;
+constexpr int kBlock = 256;
+
+struct SceneDev {
+    int n;             // cells per axis
+    int n_forces;
+    int n_spheres;
+    int frame;         // FlipSim::m_frame (advanced by the BEGIN stage)
+    float maxd;        // (float)n
+    float density;     // lattice spacing in cells (m_density)
+    float dt;          // m_stepsize
+    float picflip;     // m_picflipratio
+    float max_density; // m_max_density (Init)
+    float dens_h;      // 4*density/maxd, ComputeDensity's Smooth radius (flip.cpp:724)
+    float sdf0;        // 0.2*(1/density^3), CellSDF's threshold (particlegrid.cpp:88-89)
+    float h;           // 1/maxd, cell width (flip.cpp:417, 573)
+    float ax_h;        // 1/(n*n), ComputeAx's divisor (solver.inl:199-200)
+    float resample_re; // density/maxd (flip.cpp:120)
+    float pushout_re;  // 1.5*density/maxd (flip.cpp:268)
+    int subcell;
+    float fdt[ARIEL_MAX_FORCES][3];  // force * dt, applied in order
+    float4 sphere[ARIEL_MAX_SPHERES]; // world units: centre xyz, radius
+    long long p_begin, p_end;
+    long long c_begin;
+    long long f_begin;
+    unsigned long long rng_seed;
+    int resample_every;  // resample on frames divisible by this (1: every step, flip.cpp:121)
+    int pad;
+};
+
+// ------------------------------------------------------------------------------------------
+// glm restatement: glm::min/max are ternaries (NaN and signed-zero behaviour included).
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
+__host__ __device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
+
+// Cell coordinate of a unit-cube position (particlegrid.cpp:156-158, flip.cpp:711-713).
+__device__ __forceinline__ int cell_coord(float maxd, float x) {
+    return (int)gmax(0.0f, gmin((float)(int)maxd - 1.0f, (float)(int)maxd * x));
+}
+
+// kernels.inl:25-38
+__device__ __forceinline__ float sqrlength(float ax, float ay, float az, float bx, float by, float bz) {
+    float a = ax - bx;
+    float b = ay - by;
+    float c = az - bz;
+    return a * a + b * b + c * c;
+}
+__device__ __forceinline__ float smooth_k(float r2, float h) { return gmax(1.0f - r2 / (h * h), 0.0f); }
+__device__ __forceinline__ float sharpen_k(float r2, float h) {
+    return gmax(h * h / gmax(r2, 1.0e-5f) - 1.0f, 0.0f);
+}
+
+// glm::dot / length / normalize as used by the solid-constraint paths.
+__device__ __forceinline__ float gdot3(float3 a, float3 b) {
+    float tx = a.x * b.x, ty = a.y * b.y, tz = a.z * b.z;
+    return (tx + ty) + tz;
+}
+__device__ __forceinline__ float glength3(float3 v) { return sqrtf(gdot3(v, v)); }
+__device__ __forceinline__ float3 gnormalize3(float3 v) {
+    float s = 1.0f / sqrtf(gdot3(v, v));
+    return make_float3(v.x * s, v.y * s, v.z * s);
+}
+__device__ __forceinline__ float3 f3add(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 f3sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 f3mul(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 f3smul(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 f3div(float3 a, float s) { return make_float3(a.x / s, a.y / s, a.z / s); }
+
+__device__ __forceinline__ int type_of(float4 v) { return __float_as_int(v.w); }
+
+// ------------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): replaces rand() of the resampler.
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        unsigned long long p0 = (unsigned long long)0xD2511F53u * c.x;
+        unsigned long long p1 = (unsigned long long)0xCD9E8D57u * c.z;
+        uint4 o;
+        o.x = (uint32_t)(p1 >> 32) ^ c.y ^ k0;
+        o.y = (uint32_t)p1;
+        o.z = (uint32_t)(p0 >> 32) ^ c.w ^ k1;
+        o.w = (uint32_t)p0;
+        c = o;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+constexpr uint32_t kTagSeed = 0x53454544u;      // "SEED"
+constexpr uint32_t kTagResample = 0x5245534Du;  // "RESM"
+
+// ------------------------------------------------------------------------------------------
+// Packed index -> scene.  `pref` holds k+1 ascending begins; a block copies it to shared
+// memory once and every thread binary-searches it.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ int find_scene(const long long* __restrict__ pref_s, int k, long long g) {
+    int lo = 0, hi = k - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (pref_s[mid] <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int MAXK>
+__device__ __forceinline__ void load_prefix(long long* dst, const long long* __restrict__ src, int k) {
+    for (int i = threadIdx.x; i <= k && i < MAXK + 1; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
+
+}  // namespace ariel

@@ -1,0 +1,1154 @@
+// host.cu -- host orchestration behind the C ABI (include/ariel.h).
+//
+// An `ariel_sim` owns k >= 1 scenes laid out over packed particle / cell / face index spaces
+// (see common.cuh).  The FlipSim step order of the reference (src/sim/flip.cpp:92-128) is
+// reproduced stage by stage; a whole step is captured once into a CUDA graph and replayed.
+// Frame counters, the resampling schedule and the pressure solve's stopping decisions all live
+// on the device, so a step needs no host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "pcg.cuh"
+
+using namespace ariel;
+
+namespace {
+
+struct DeviceBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+thread_local char g_last_error[256] = "";
+
+#define ARIEL_CUDA(call)                                                        \
+    do {                                                                        \
+        cudaError_t e_ = (call);                                                \
+        if (e_ != cudaSuccess) return map_cuda_error(e_, #call);                \
+    } while (0)
+
+ariel_status map_cuda_error(cudaError_t e, const char* what = "") {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return ARIEL_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ARIEL_ERR_NO_DEVICE;
+    return ARIEL_ERR_CUDA;
+}
+
+// Every copy goes through the handle's stream (non-blocking, so the legacy default stream would
+// not be ordered with the kernels) and is waited for before returning.
+cudaError_t copy_sync(cudaStream_t st, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
+// Host copy of the per-scene particle arrays (id order) used while (re)building packed state.
+struct HostParticles {
+    std::vector<float4> pos4;  // x y z mass
+    std::vector<float4> vel4;  // u v w type-bits
+};
+
+inline float4 pack_vel(float u, float v, float w, int type) {
+    float4 r;
+    r.x = u;
+    r.y = v;
+    r.z = w;
+    int t = type;
+    std::memcpy(&r.w, &t, 4);
+    return r;
+}
+inline int type_bits(const float4& v) {
+    int t;
+    std::memcpy(&t, &v.w, 4);
+    return t;
+}
+
+inline float hmin(float x, float y) { return (y < x) ? y : x; }  // glm::min
+inline float hmax(float x, float y) { return (x < y) ? y : x; }  // glm::max
+
+// Scene::GenerateParticles (src/scene/scene.cpp:257-360) for box liquids and analytic sphere
+// solids, placed in lexicographic (i,j,k) lattice order: liquid particles first, then solids
+// (scene.cpp:349-354).  Liquid particles may be jittered inside their lattice sub-cell by
+// Philox4x32-10 keyed by (seed, particle index, box).
+void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
+    const int n = d.dim;
+    const float maxdim = (float)n;
+    const float thickness = 1.0f / maxdim;
+    const float density = d.density;
+    const float w = density * thickness;
+    const uint32_t k0 = (uint32_t)d.seed, k1 = (uint32_t)(d.seed >> 32);
+    auto inside_solid = [&](float x, float y, float z) {
+        for (int s = 0; s < d.n_solid; ++s) {
+            float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
+                  cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
+            float dx = x - cx, dy = y - cy, dz = z - cz;
+            float dd = (dx * dx + dy * dy) + dz * dz;
+            if (dd < r * r) return true;
+        }
+        return false;
+    };
+    out.pos4.clear();
+    out.vel4.clear();
+    for (int l = 0; l < d.n_liquid; ++l) {
+        const AsimBox& bx = d.liquid[l];
+        float lminx = hmax(std::floor(bx.lo[0] * maxdim), 0.0f) / density;
+        float lminy = hmax(std::floor(bx.lo[1] * maxdim), 0.0f) / density;
+        float lminz = hmax(std::floor(bx.lo[2] * maxdim), 0.0f) / density;
+        float lmaxx = hmin(std::ceil(bx.hi[0] * maxdim), maxdim + 1.0f) / density;
+        float lmaxy = hmin(std::ceil(bx.hi[1] * maxdim), maxdim + 1.0f) / density;
+        float lmaxz = hmin(std::ceil(bx.hi[2] * maxdim), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    float cx = (i * w) + (w / 2.0f), cy = (j * w) + (w / 2.0f), cz = (k * w) + (w / 2.0f);
+                    float wx = cx * maxdim, wy = cy * maxdim, wz = cz * maxdim;
+                    bool inside = wx > bx.lo[0] * maxdim && wx < bx.hi[0] * maxdim && wy > bx.lo[1] * maxdim &&
+                                  wy < bx.hi[1] * maxdim && wz > bx.lo[2] * maxdim && wz < bx.hi[2] * maxdim;
+                    if (!inside || inside_solid(wx, wy, wz)) continue;
+                    float px = cx, py = cy, pz = cz;
+                    if (d.jitter > 0.0f) {
+                        uint32_t id = (uint32_t)out.pos4.size();
+                        uint4 rv = philox4x32_10(make_uint4(id, (uint32_t)l, 0u, kTagSeed), k0, k1);
+                        float ux = (float)(rv.x >> 8) * (1.0f / 16777216.0f);
+                        float uy = (float)(rv.y >> 8) * (1.0f / 16777216.0f);
+                        float uz = (float)(rv.z >> 8) * (1.0f / 16777216.0f);
+                        px = (i * w) + (ux * w);
+                        py = (j * w) + (uy * w);
+                        pz = (k * w) + (uz * w);
+                    }
+                    out.pos4.push_back(make_float4(px, py, pz, 1.0f));
+                    out.vel4.push_back(pack_vel(bx.vel[0], bx.vel[1], bx.vel[2], ARIEL_FLUID));
+                }
+    }
+    for (int s = 0; s < d.n_solid; ++s) {
+        float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
+              cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
+        float lminx = hmax(std::floor(cx - r), 0.0f) / density;
+        float lminy = hmax(std::floor(cy - r), 0.0f) / density;
+        float lminz = hmax(std::floor(cz - r), 0.0f) / density;
+        float lmaxx = hmin(std::ceil(cx + r), maxdim + 1.0f) / density;
+        float lmaxy = hmin(std::ceil(cy + r), maxdim + 1.0f) / density;
+        float lmaxz = hmin(std::ceil(cz + r), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    float px = (i * w) + (w / 2.0f), py = (j * w) + (w / 2.0f), pz = (k * w) + (w / 2.0f);
+                    float wx = px * maxdim - cx, wy = py * maxdim - cy, wz = pz * maxdim - cz;
+                    float dd = (wx * wx + wy * wy) + wz * wz;
+                    if (!(dd < r * r)) continue;
+                    out.pos4.push_back(make_float4(px, py, pz, 10.0f));
+                    out.vel4.push_back(pack_vel(0.0f, 0.0f, 0.0f, ARIEL_SOLID));
+                }
+    }
+}
+
+// FlipSim::Init's density normaliser (flip.cpp:42-70): density of a 10x10x10 lattice of
+// unit-mass FLUID particles at spacing density/maxd, max over the lattice.  One block per
+// scene; each particle gathers the lattice particles of its 27 cells in cell order, then in
+// particle order inside a cell -- the order ParticleGrid::Sort gives them.
+__global__ void k_max_density(SceneDev* scenes, int k) {
+    const int s = blockIdx.x;
+    if (s >= k) return;
+    SceneDev& D = scenes[s];
+    __shared__ float px[1000], py[1000], pz[1000];
+    __shared__ int pc[1000];
+    __shared__ float best[1024];
+    const float maxd = D.maxd;
+    const float h = D.density / maxd;
+    const int n = D.n;
+    for (int t = threadIdx.x; t < 1000; t += blockDim.x) {
+        int i = t / 100, j = (t / 10) % 10, kk = t % 10;
+        px[t] = ((float)i + 0.5f) * h;
+        py[t] = ((float)j + 0.5f) * h;
+        pz[t] = ((float)kk + 0.5f) * h;
+        int ci = cell_coord(maxd, px[t]), cj = cell_coord(maxd, py[t]), ck = cell_coord(maxd, pz[t]);
+        pc[t] = (ci * n + cj) * n + ck;
+    }
+    __syncthreads();
+    float dens = 0.0f;
+    const int t = threadIdx.x;
+    if (t < 1000) {
+        int ci = cell_coord(maxd, px[t]), cj = cell_coord(maxd, py[t]), ck = cell_coord(maxd, pz[t]);
+        const float hk = D.dens_h;
+        float weightsum = 0.0f;
+        for (int sx = ci - 1; sx <= ci + 1; ++sx) {
+            if (sx < 0 || sx > n - 1) continue;
+            for (int sy = cj - 1; sy <= cj + 1; ++sy) {
+                if (sy < 0 || sy > n - 1) continue;
+                for (int sz = ck - 1; sz <= ck + 1; ++sz) {
+                    if (sz < 0 || sz > n - 1) continue;
+                    int cell = (sx * n + sy) * n + sz;
+                    for (int m = 0; m < 1000; ++m) {
+                        if (pc[m] != cell) continue;
+                        float sqd = sqrlength(px[m], py[m], pz[m], px[t], py[t], pz[t]);
+                        float weight = 1.0f * smooth_k(sqd, hk);
+                        weightsum = weightsum + weight;
+                    }
+                }
+            }
+        }
+        dens = weightsum / 1.0f;
+    }
+    best[t] = t < 1000 ? dens : 0.0f;
+    __syncthreads();
+    if (t == 0) {
+        float m = 0.0f;
+        for (int i = 0; i < 1000; ++i) m = gmax(m, best[i]);
+        D.max_density = m;
+    }
+}
+
+}  // namespace
+
+constexpr int kEvSolveKernel = ARIEL_STAGE_COUNT + 1;
+constexpr int kEvCount = ARIEL_STAGE_COUNT + 2;
+
+struct ariel_sim {
+    int device = 0;
+    int k = 0;
+    std::vector<AsimSceneDesc> descs;
+    AsimParams prm{};
+    std::vector<SceneDev> sh;  // host mirror of the scene table
+    std::vector<long long> ppref, cpref, fpref;
+    long long np = 0, nc = 0, nf = 0;
+    bool any_solid = false;
+    bool inited = false;
+    cudaStream_t stream = nullptr;
+    std::vector<DeviceBuf> bufs;
+    // device pointers
+    SceneDev* d_scenes = nullptr;
+    long long *d_ppref = nullptr, *d_cpref = nullptr, *d_fpref = nullptr;
+    DevState S{};
+    PcgArgs PA{};
+    void* scan_tmp = nullptr;
+    uint32_t *flpred = nullptr, *flscan = nullptr;
+    float* d_dens_id = nullptr;
+    int pcg_blocks = 0;
+    int mode = kRef32;
+    // graphs of one whole step: [0] plain, [1],[2] with the two stage-event sets
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+    bool graph_tried[3] = {false, false, false};
+    long long graph_kernels[3] = {0, 0, 0};
+    // timing: two event sets (stage boundaries + solve-kernel start), used alternately so that
+    // one step's events are read while the next step runs
+    cudaEvent_t ev[2][kEvCount] = {};
+    bool ev_pending[2] = {false, false};
+    int ev_slot = 0;
+    double acc_stage[ARIEL_STAGE_COUNT] = {};
+    double acc_solve_kernel = 0;
+    std::vector<double> step_hist;
+    cudaEvent_t tb = nullptr, te = nullptr;
+    double stage_ms[ARIEL_STAGE_COUNT] = {};
+    double step_ms = 0;
+    float* d_stage = nullptr;  // xyz staging for host-buffer particle I/O
+    int last_status = ARIEL_OK;
+    std::vector<int64_t> frames;
+};
+
+namespace {
+
+template <class T>
+ariel_status dalloc(ariel_sim* s, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ARIEL_ERR_OOM;
+    }
+    s->bufs.push_back(DeviceBuf{q, count * sizeof(T)});
+    *p = (T*)q;
+    return ARIEL_OK;
+}
+
+void free_all(ariel_sim* s) {
+    for (int i = 0; i < 3; ++i) {
+        if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
+        s->graph[i] = nullptr;
+        s->graph_tried[i] = false;
+    }
+    for (auto& b : s->bufs) cudaFree(b.p);
+    s->bufs.clear();
+}
+
+#define ARIEL_TRY(x)                          \
+    do {                                      \
+        ariel_status st_ = (x);               \
+        if (st_ != ARIEL_OK) return st_;      \
+    } while (0)
+
+SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
+    SceneDev D{};
+    D.n = d.dim;
+    D.n_forces = d.n_forces;
+    D.n_spheres = d.n_solid;
+    D.frame = 0;
+    D.maxd = (float)d.dim;
+    D.density = d.density;
+    D.dt = d.stepsize;
+    D.picflip = p.picflip;
+    D.max_density = 1.0f;
+    D.dens_h = 4.0f * d.density / D.maxd;
+    float n0 = 1.0f / (d.density * d.density * d.density);
+    D.sdf0 = 0.2f * n0;
+    D.h = 1.0f / D.maxd;
+    float nn = (float)d.dim;
+    D.ax_h = 1.0f / (nn * nn);
+    D.resample_re = d.density / D.maxd;
+    D.pushout_re = 1.5f * d.density / D.maxd;
+    D.subcell = p.subcell;
+    for (int j = 0; j < d.n_forces && j < ARIEL_MAX_FORCES; ++j)
+        for (int a = 0; a < 3; ++a) D.fdt[j][a] = d.forces[j][a] * d.stepsize;
+    for (int i = 0; i < d.n_solid && i < ARIEL_MAX_SPHERES; ++i)
+        D.sphere[i] = make_float4(d.solid[i].center[0] * D.maxd, d.solid[i].center[1] * D.maxd,
+                                  d.solid[i].center[2] * D.maxd, d.solid[i].radius * D.maxd);
+    D.rng_seed = p.rng_seed;
+    D.resample_every = p.resample_every;
+    return D;
+}
+
+ariel_status validate(const AsimSceneDesc& d) {
+    if (d.dim < 2 || d.dim > 1024) return ARIEL_ERR_INVALID_ARG;
+    if (!(d.density > 0.0f) || !(d.stepsize > 0.0f)) return ARIEL_ERR_INVALID_ARG;
+    if (d.n_forces < 0 || d.n_forces > ARIEL_MAX_FORCES) return ARIEL_ERR_INVALID_ARG;
+    if (d.n_liquid < 0 || d.n_liquid > ARIEL_MAX_BOXES) return ARIEL_ERR_INVALID_ARG;
+    if (d.n_solid < 0 || d.n_solid > ARIEL_MAX_SPHERES) return ARIEL_ERR_INVALID_ARG;
+    if ((long long)d.dim * d.dim * d.dim > (1ll << 30)) return ARIEL_ERR_INVALID_ARG;
+    return ARIEL_OK;
+}
+
+// (Re)allocate every buffer for the current scene list and particle counts, upload the
+// particles given per scene, and bin the static SOLID particles.
+ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
+    free_all(s);
+    const int k = s->k;
+    s->ppref.assign(k + 1, 0);
+    s->cpref.assign(k + 1, 0);
+    s->fpref.assign(k + 1, 0);
+    s->any_solid = false;
+    for (int i = 0; i < k; ++i) {
+        long long n = s->descs[i].dim;
+        s->ppref[i + 1] = s->ppref[i] + (long long)hp[i].pos4.size();
+        s->cpref[i + 1] = s->cpref[i] + n * n * n;
+        s->fpref[i + 1] = s->fpref[i] + 3 * n * n * (n + 1);
+        s->sh[i].p_begin = s->ppref[i];
+        s->sh[i].p_end = s->ppref[i + 1];
+        s->sh[i].c_begin = s->cpref[i];
+        s->sh[i].f_begin = s->fpref[i];
+        if (s->descs[i].n_solid > 0) s->any_solid = true;
+    }
+    s->np = s->ppref[k];
+    s->nc = s->cpref[k];
+    s->nf = s->fpref[k];
+    if (s->np >= (1ll << 31) || s->nc >= (1ll << 31)) return ARIEL_ERR_INVALID_ARG;
+    const long long np = s->np, nc = s->nc, nf = s->nf;
+    DevState& S = s->S;
+    S = DevState{};
+    S.k = k;
+    S.any_solid = s->any_solid;
+    S.np = np;
+    S.nc = nc;
+    S.nf = nf;
+    ARIEL_TRY(dalloc(s, &s->d_scenes, k));
+    ARIEL_TRY(dalloc(s, &s->d_ppref, k + 1));
+    ARIEL_TRY(dalloc(s, &s->d_cpref, k + 1));
+    ARIEL_TRY(dalloc(s, &s->d_fpref, k + 1));
+    S.scenes = s->d_scenes;
+    S.p_pref = s->d_ppref;
+    S.c_pref = s->d_cpref;
+    S.f_pref = s->d_fpref;
+    ARIEL_TRY(dalloc(s, &S.pos4, np));
+    ARIEL_TRY(dalloc(s, &S.vel4, np));
+    if (s->any_solid) {
+        ARIEL_TRY(dalloc(s, &S.pt4, np));
+        ARIEL_TRY(dalloc(s, &S.ut4, np));
+    }
+    ARIEL_TRY(dalloc(s, &S.key, np));
+    ARIEL_TRY(dalloc(s, &S.off, np));
+    ARIEL_TRY(dalloc(s, &S.count, nc));
+    ARIEL_TRY(dalloc(s, &S.start, nc + 1));
+    ARIEL_TRY(dalloc(s, &S.sid, np));
+    ARIEL_TRY(dalloc(s, &S.spos4, np));
+    ARIEL_TRY(dalloc(s, &S.svel4, np));
+    ARIEL_TRY(dalloc(s, &S.dens, np));
+    ARIEL_TRY(dalloc(s, &s->d_dens_id, np));
+    ARIEL_TRY(dalloc(s, &s->d_stage, 6 * (size_t)np));
+    ARIEL_TRY(dalloc(s, &S.solid_start, nc + 1));
+    ARIEL_TRY(dalloc(s, &S.flags, nc));
+    ARIEL_TRY(dalloc(s, &S.L, nc));
+    ARIEL_TRY(dalloc(s, &S.D, nc));
+    ARIEL_TRY(dalloc(s, &S.P, nc));
+    ARIEL_TRY(dalloc(s, &S.P64, nc));
+    ARIEL_TRY(dalloc(s, &S.u, nf));
+    ARIEL_TRY(dalloc(s, &S.pu, nf));
+    ARIEL_TRY(dalloc(s, &S.dev_error, 1));
+    size_t st_bytes = scan_tmp_bytes(nc);
+    char* tmp = nullptr;
+    ARIEL_TRY(dalloc(s, &tmp, st_bytes));
+    s->scan_tmp = tmp;
+    // pressure solve
+    PcgArgs& A = s->PA;
+    A = PcgArgs{};
+    s->mode = s->prm.precision == ARIEL_PREC_FP64 ? kFp64 : (s->prm.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
+    A.mode = s->mode;
+    A.precond = s->prm.precond;
+    A.stop_rule = s->prm.stop_rule;
+    A.max_iters = s->prm.max_iters;
+    A.max_outer = s->prm.max_outer > 0 ? s->prm.max_outer : 8;
+    A.chunk = 1024;
+    A.tol = s->prm.tol;
+    A.inner_tol = s->prm.inner_tol > 0 ? s->prm.inner_tol : 1e-4;
+    A.tau = s->prm.mic_tau;
+    A.sigma = s->prm.mic_sigma;
+    double tmo_ms = s->prm.barrier_timeout_ms > 0 ? s->prm.barrier_timeout_ms : 2000.0;
+    A.timeout_ns = (unsigned long long)(tmo_ms * 1.0e6);
+    uint32_t* fl = nullptr;
+    long long *flp = nullptr, *chp = nullptr;
+    ARIEL_TRY(dalloc(s, &fl, nc));
+    ARIEL_TRY(dalloc(s, &flp, k + 1));
+    ARIEL_TRY(dalloc(s, &chp, k + 1));
+    A.fl = fl;
+    A.fl_pref = flp;
+    A.ch_pref = chp;
+    ARIEL_TRY(dalloc(s, &s->flpred, nc));
+    ARIEL_TRY(dalloc(s, &s->flscan, nc + 1));
+    ARIEL_TRY(dalloc(s, &A.mask, nc));
+    ARIEL_TRY(dalloc(s, &A.diag, nc));
+    ARIEL_TRY(dalloc(s, &A.pc64, nc));
+    ARIEL_TRY(dalloc(s, &A.pc32, nc));
+    const size_t vb = s->mode == kFp64 ? 8 : 4;
+    char* v[6];
+    for (int i = 0; i < 6; ++i) ARIEL_TRY(dalloc(s, &v[i], vb * (size_t)nc));
+    A.r = v[0];
+    A.z = v[1];
+    A.s0 = v[2];
+    A.s1 = v[3];
+    A.q = v[4];
+    A.ordq = v[5];
+    if (s->mode == kMixed) {
+        ARIEL_TRY(dalloc(s, &A.r64, nc));
+        ARIEL_TRY(dalloc(s, &A.d32, nc));
+    }
+    long long maxch = 0;
+    for (int i = 0; i < k; ++i) {
+        long long n = s->descs[i].dim;
+        maxch += (n * n * n + A.chunk - 1) / A.chunk;
+    }
+    A.max_chunks = std::max(1ll, maxch);
+    ARIEL_TRY(dalloc(s, &A.partial, 2 * A.max_chunks));
+    ARIEL_TRY(dalloc(s, &A.sc, k));
+    ARIEL_TRY(dalloc(s, &A.totals, k));
+    ARIEL_CUDA(cudaMemsetAsync(A.totals, 0, sizeof(PcgTotals) * k, s->stream));
+    ARIEL_TRY(dalloc(s, &A.ctl, 1));
+    ARIEL_TRY(dalloc(s, &A.bar, 1));
+    A.S = S;
+    s->pcg_blocks = pcg_max_blocks(s->device, s->mode);
+    // uploads
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_scenes, s->sh.data(), sizeof(SceneDev) * k, cudaMemcpyHostToDevice, s->stream));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_ppref, s->ppref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_cpref, s->cpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_fpref, s->fpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
+    for (int i = 0; i < k; ++i) {
+        size_t cnt = hp[i].pos4.size();
+        if (cnt == 0) continue;
+        ARIEL_CUDA(copy_sync(s->stream, S.pos4 + s->ppref[i], hp[i].pos4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
+        ARIEL_CUDA(copy_sync(s->stream, S.vel4 + s->ppref[i], hp[i].vel4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
+    }
+    ARIEL_CUDA(cudaMemsetAsync(S.P, 0, sizeof(float) * nc, s->stream));
+    ARIEL_CUDA(cudaMemsetAsync(S.P64, 0, sizeof(double) * nc, s->stream));
+    ARIEL_CUDA(cudaMemsetAsync(S.dev_error, 0, sizeof(int), s->stream));
+    ARIEL_CUDA(cudaMemsetAsync(S.u, 0, sizeof(float) * nf, s->stream));
+    ARIEL_CUDA(cudaMemsetAsync(S.pu, 0, sizeof(float) * nf, s->stream));
+    ARIEL_CUDA(cudaMemsetAsync(S.flags, 0, nc, s->stream));
+    // static SOLID particles binned by cell, id order inside a cell (positions never change:
+    // only FLUID particles are moved by any stage of the step)
+    std::vector<uint32_t> sstart(nc + 1, 0);
+    std::vector<std::pair<long long, float4>> sol;
+    for (int i = 0; i < k; ++i) {
+        const long long n = s->descs[i].dim;
+        const float maxd = (float)n;
+        for (size_t p = 0; p < hp[i].pos4.size(); ++p) {
+            if (type_bits(hp[i].vel4[p]) != ARIEL_SOLID) continue;
+            const float4& q = hp[i].pos4[p];
+            auto cc = [&](float x) { return (long long)(int)hmax(0.0f, hmin((float)(int)maxd - 1.0f, (float)(int)maxd * x)); };
+            long long c = s->cpref[i] + (cc(q.x) * n + cc(q.y)) * n + cc(q.z);
+            sol.push_back({c, q});
+        }
+    }
+    std::stable_sort(sol.begin(), sol.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<float4> spos(sol.size());
+    for (size_t i = 0; i < sol.size(); ++i) {
+        sstart[sol[i].first + 1]++;
+        spos[i] = sol[i].second;
+    }
+    for (long long c = 0; c < nc; ++c) sstart[c + 1] += sstart[c];
+    ARIEL_TRY(dalloc(s, &S.solid_pos, spos.size()));
+    if (!spos.empty())
+        ARIEL_CUDA(copy_sync(s->stream, S.solid_pos, spos.data(), spos.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    ARIEL_CUDA(copy_sync(s->stream, S.solid_start, sstart.data(), sstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    s->PA.S = S;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return ARIEL_OK;
+}
+
+ariel_status check_device_error(ariel_sim* s) {
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, s->S.dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    if (err & 1) return ARIEL_ERR_DEVICE_TIMEOUT;
+    if (err & 2) {
+        // non-finite uploaded state: report once
+        cudaMemsetAsync(s->S.dev_error, 0, sizeof(int), s->stream);
+        return ARIEL_ERR_NAN;
+    }
+    return ARIEL_OK;
+}
+
+ariel_status enqueue_stage(ariel_sim* s, int g, cudaEvent_t* evs = nullptr) {
+    const DevState& S = s->S;
+    cudaStream_t st = s->stream;
+    cudaError_t e = cudaSuccess;
+    switch (g) {
+        case ARIEL_STAGE_BEGIN: e = launch_begin(S, st); break;
+        case ARIEL_STAGE_SORT: e = launch_sort(S, s->scan_tmp, st); break;
+        case ARIEL_STAGE_DENSITY: e = launch_density(S, st); break;
+        case ARIEL_STAGE_FORCES: e = launch_forces(S, st); break;
+        case ARIEL_STAGE_P2G: e = launch_p2g(S, st); break;
+        case ARIEL_STAGE_CLASSIFY: e = launch_classify(S, 0, st); break;
+        case ARIEL_STAGE_BOUNDARY_DIV: e = launch_boundary_div(S, st); break;
+        case ARIEL_STAGE_SOLVE:
+            e = launch_pcg_prepare(s->PA, s->flpred, s->flscan, s->scan_tmp, st);
+            if (e == cudaSuccess && evs) e = cudaEventRecordWithFlags(evs[kEvSolveKernel], st, cudaEventRecordExternal);
+            if (e == cudaSuccess) e = launch_pcg_solve(s->PA, s->pcg_blocks, st);
+            break;
+        case ARIEL_STAGE_GRADIENT: e = launch_gradient(S, st); break;
+        case ARIEL_STAGE_EXTRAPOLATE: e = launch_extrapolate(S, st); break;
+        case ARIEL_STAGE_G2P_ADVECT: e = launch_g2p_advect(S, st); break;
+        case ARIEL_STAGE_RESAMPLE: e = launch_resample(S, s->scan_tmp, st); break;
+        default: return ARIEL_ERR_INVALID_ARG;
+    }
+    if (e != cudaSuccess) return map_cuda_error(e, "stage launch");
+    return ARIEL_OK;
+}
+
+// One step; with `evs` the stage boundaries (and the solve kernel's start) are recorded.
+ariel_status enqueue_step(ariel_sim* s, cudaEvent_t* evs) {
+    for (int g = 0; g < ARIEL_STAGE_COUNT; ++g) {
+        if (evs) ARIEL_CUDA(cudaEventRecordWithFlags(evs[g], s->stream, cudaEventRecordExternal));
+        ARIEL_TRY(enqueue_stage(s, g, evs));
+    }
+    if (evs) ARIEL_CUDA(cudaEventRecordWithFlags(evs[ARIEL_STAGE_COUNT], s->stream, cudaEventRecordExternal));
+    return ARIEL_OK;
+}
+
+// Reads a finished step's events into the accumulators.
+ariel_status collect_step_events(ariel_sim* s, int slot) {
+    cudaEvent_t* evs = s->ev[slot];
+    ARIEL_CUDA(cudaEventSynchronize(evs[ARIEL_STAGE_COUNT]));
+    for (int g = 0; g < ARIEL_STAGE_COUNT; ++g) {
+        float ms = 0;
+        ARIEL_CUDA(cudaEventElapsedTime(&ms, evs[g], evs[g + 1]));
+        s->stage_ms[g] = ms;
+        s->acc_stage[g] += ms;
+    }
+    float ks = 0, tot = 0;
+    ARIEL_CUDA(cudaEventElapsedTime(&ks, evs[kEvSolveKernel], evs[ARIEL_STAGE_SOLVE + 1]));
+    ARIEL_CUDA(cudaEventElapsedTime(&tot, evs[0], evs[ARIEL_STAGE_COUNT]));
+    s->acc_solve_kernel += ks;
+    s->step_ms = tot;
+    s->step_hist.push_back(tot);
+    s->ev_pending[slot] = false;
+    return ARIEL_OK;
+}
+
+// which: 0 plain step, 1/2 step recording event set 0/1.
+void try_build_graph(ariel_sim* s, int which) {
+    s->graph_tried[which] = true;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    long long before = launch_count();
+    ariel_status st = enqueue_step(s, which == 0 ? nullptr : s->ev[which - 1]);
+    long long kernels = launch_count() - before;
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != ARIEL_OK || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return;
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    s->graph[which] = ex;
+    s->graph_kernels[which] = kernels;
+    count_launch(-(int)kernels);  // capture does not launch; replays are counted instead
+}
+
+ariel_status sort_and_classify_init(ariel_sim* s) {
+    cudaError_t e = launch_sort(s->S, s->scan_tmp, s->stream);
+    if (e == cudaSuccess) e = launch_fill_dens(s->S, 10.0f, s->stream);  // AddLiquidParticle: m_density = 10
+    if (e == cudaSuccess) e = launch_classify(s->S, 1, s->stream);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    return ARIEL_OK;
+}
+
+ariel_status download_particles(ariel_sim* s, std::vector<HostParticles>& hp) {
+    hp.assign(s->k, HostParticles{});
+    for (int i = 0; i < s->k; ++i) {
+        long long b = s->ppref[i], n = s->ppref[i + 1] - b;
+        hp[i].pos4.resize(n);
+        hp[i].vel4.resize(n);
+        if (n == 0) continue;
+        ARIEL_CUDA(copy_sync(s->stream, hp[i].pos4.data(), s->S.pos4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+        ARIEL_CUDA(copy_sync(s->stream, hp[i].vel4.data(), s->S.vel4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
+    return ARIEL_OK;
+}
+
+ariel_status create_common(const AsimSceneDesc* descs, int32_t k, const AsimParams* params, ariel_sim** out) {
+    if (!descs || !params || !out || k < 1 || k > kMaxScenes) return ARIEL_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (int i = 0; i < k; ++i) ARIEL_TRY(validate(descs[i]));
+    if (params->precision < 0 || params->precision > 2 || params->precond < 0 || params->precond > 1 ||
+        params->stop_rule < 0 || params->stop_rule > 1)
+        return ARIEL_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return ARIEL_ERR_NO_DEVICE;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return ARIEL_ERR_NO_DEVICE;  // built for sm_100a only
+    ariel_sim* s = new (std::nothrow) ariel_sim();
+    if (!s) return ARIEL_ERR_OOM;
+    s->device = dev;
+    s->k = k;
+    s->descs.assign(descs, descs + k);
+    s->prm = *params;
+    s->frames.assign(k, 0);
+    for (int i = 0; i < k; ++i) s->sh.push_back(make_scene(descs[i], *params));
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return ARIEL_ERR_CUDA;
+    }
+    for (auto& set : s->ev)
+        for (auto& e : set) cudaEventCreate(&e);
+    cudaEventCreate(&s->tb);
+    cudaEventCreate(&s->te);
+    std::vector<HostParticles> empty(k);
+    ariel_status st = build_state(s, empty);
+    if (st != ARIEL_OK) {
+        free_all(s);
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return st;
+    }
+    *out = s;
+    return ARIEL_OK;
+}
+
+}  // namespace
+
+// ==============================================================================================
+// C ABI
+// ==============================================================================================
+extern "C" {
+
+int32_t ariel_abi_version(void) { return ARIEL_ABI_VERSION; }
+
+void ariel_params_default(AsimParams* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->picflip = 0.95f;  // flip.cpp:27
+    p->subcell = 1;      // flip.cpp:26
+    p->precond = ARIEL_PRECOND_REF;
+    p->precision = ARIEL_PREC_REF32;
+    p->stop_rule = ARIEL_STOP_REF_ABS;
+    p->max_iters = 0;
+    p->tol = 1e-5;
+    p->inner_tol = 1e-4;
+    p->max_outer = 8;
+    p->resample_every = 1;  // flip.cpp:121
+    p->mic_tau = 0.97;
+    p->mic_sigma = 0.25;
+    p->rng_seed = 0x5EED;
+    p->use_graph = 1;
+    p->timing = 0;
+    p->barrier_timeout_ms = 2000.0;
+    p->fail_on_not_converged = 0;
+}
+
+void ariel_scene_dambreak(AsimSceneDesc* d, int32_t n) {
+    if (!d) return;
+    std::memset(d, 0, sizeof(*d));
+    d->dim = n;
+    d->density = 0.5f;
+    d->stepsize = 1.0f / 240.0f;
+    d->n_forces = 1;
+    d->forces[0][1] = -9.8f;
+    d->n_liquid = 1;
+    d->liquid[0].hi[0] = 0.4f;
+    d->liquid[0].hi[1] = 0.6f;
+    d->liquid[0].hi[2] = 1.0f;
+    d->seed = 1;
+    d->jitter = 1.0f;
+}
+
+const char* ariel_status_string(ariel_status st) {
+    switch (st) {
+        case ARIEL_OK: return "ok";
+        case ARIEL_ERR_INVALID_ARG: return "invalid argument";
+        case ARIEL_ERR_OOM: return "device memory exhausted";
+        case ARIEL_ERR_NOT_CONVERGED: return "pressure solve did not converge";
+        case ARIEL_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case ARIEL_ERR_CUDA: return "CUDA error";
+        case ARIEL_ERR_STATE: return "call out of order";
+        case ARIEL_ERR_NO_DEVICE: return "no sm_100 device";
+        case ARIEL_ERR_NAN: return "non-finite input";
+    }
+    return "unknown status";
+}
+
+ariel_status ariel_create(const AsimSceneDesc* desc, const AsimParams* params, ariel_sim** out) {
+    return create_common(desc, 1, params, out);
+}
+
+ariel_status ariel_create_batch(const AsimSceneDesc* descs, int32_t k, const AsimParams* params, ariel_sim** out) {
+    return create_common(descs, k, params, out);
+}
+
+ariel_status ariel_destroy(ariel_sim* s) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    cudaStreamSynchronize(s->stream);
+    free_all(s);
+    for (auto& set : s->ev)
+        for (auto& e : set) cudaEventDestroy(e);
+    cudaEventDestroy(s->tb);
+    cudaEventDestroy(s->te);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_scene_count(ariel_sim* s, int32_t* k) {
+    if (!s || !k) return ARIEL_ERR_INVALID_ARG;
+    *k = s->k;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_init(ariel_sim* s) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    // m_max_density from the 10^3 lattice, per scene (flip.cpp:47-70)
+    k_max_density<<<s->k, 1024, 0, s->stream>>>(s->d_scenes, s->k);
+    count_launch();
+    ARIEL_CUDA(cudaGetLastError());
+    std::vector<SceneDev> dev(s->k);
+    ARIEL_CUDA(cudaMemcpyAsync(dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost, s->stream));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < s->k; ++i) {
+        s->sh[i].max_density = dev[i].max_density;
+        s->sh[i].frame = 0;
+        s->frames[i] = 0;
+    }
+    std::vector<HostParticles> hp(s->k);
+    for (int i = 0; i < s->k; ++i) generate_particles(s->descs[i], hp[i]);
+    ARIEL_TRY(build_state(s, hp));
+    ARIEL_TRY(sort_and_classify_init(s));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    s->inited = true;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_set_particles(ariel_sim* s, int32_t scene, int64_t n, const float* pos, const float* vel,
+                                 const float* mass, const int32_t* type) {
+    if (!s || scene < 0 || scene >= s->k || n < 0 || (n > 0 && (!pos || !vel || !mass || !type)))
+        return ARIEL_ERR_INVALID_ARG;
+    for (int64_t i = 0; i < 3 * n; ++i)
+        if (!std::isfinite(pos[i]) || !std::isfinite(vel[i])) return ARIEL_ERR_NAN;
+    cudaStreamSynchronize(s->stream);
+    std::vector<SceneDev> dev(s->k);
+    ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < s->k; ++i) {
+        s->sh[i].frame = dev[i].frame;
+        s->sh[i].max_density = dev[i].max_density;
+    }
+    std::vector<HostParticles> hp;
+    ARIEL_TRY(download_particles(s, hp));
+    hp[scene].pos4.resize(n);
+    hp[scene].vel4.resize(n);
+    for (int64_t i = 0; i < n; ++i) {
+        hp[scene].pos4[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], mass[i]);
+        hp[scene].vel4[i] = pack_vel(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], type[i]);
+    }
+    // keep the pressure warm start of every scene
+    std::vector<float> P(s->nc);
+    std::vector<double> P64(s->nc);
+    ARIEL_CUDA(copy_sync(s->stream, P.data(), s->S.P, sizeof(float) * s->nc, cudaMemcpyDeviceToHost));
+    ARIEL_CUDA(copy_sync(s->stream, P64.data(), s->S.P64, sizeof(double) * s->nc, cudaMemcpyDeviceToHost));
+    ARIEL_TRY(build_state(s, hp));
+    ARIEL_CUDA(copy_sync(s->stream, s->S.P, P.data(), sizeof(float) * s->nc, cudaMemcpyHostToDevice));
+    ARIEL_CUDA(copy_sync(s->stream, s->S.P64, P64.data(), sizeof(double) * s->nc, cudaMemcpyHostToDevice));
+    if (!s->inited) {
+        // a handle fed directly with particles still needs the density normaliser
+        k_max_density<<<s->k, 1024, 0, s->stream>>>(s->d_scenes, s->k);
+        count_launch();
+        ARIEL_CUDA(cudaGetLastError());
+        ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < s->k; ++i) s->sh[i].max_density = dev[i].max_density;
+        s->inited = true;
+    }
+    ARIEL_TRY(sort_and_classify_init(s));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return ARIEL_OK;
+}
+
+ariel_status ariel_stage(ariel_sim* s, int32_t stage) {
+    if (!s || stage < 0 || stage >= ARIEL_STAGE_COUNT) return ARIEL_ERR_INVALID_ARG;
+    if (!s->inited) return ARIEL_ERR_STATE;
+    if (stage == ARIEL_STAGE_BEGIN)
+        for (auto& f : s->frames) f++;
+    ARIEL_TRY(enqueue_stage(s, stage));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
+}
+
+ariel_status ariel_step(ariel_sim* s, int32_t nsteps) {
+    if (!s || nsteps < 0) return ARIEL_ERR_INVALID_ARG;
+    if (!s->inited) return ARIEL_ERR_STATE;
+    const bool timed = s->prm.timing != 0;
+    for (int it = 0; it < nsteps; ++it) {
+        if (timed) {
+            const int slot = s->ev_slot;
+            s->ev_slot ^= 1;
+            if (s->ev_pending[slot]) ARIEL_TRY(collect_step_events(s, slot));
+            if (s->prm.use_graph && !s->graph_tried[1 + slot]) try_build_graph(s, 1 + slot);
+            if (s->graph[1 + slot]) {
+                cudaError_t e = cudaGraphLaunch(s->graph[1 + slot], s->stream);
+                if (e != cudaSuccess) return map_cuda_error(e);
+                count_launch((int)s->graph_kernels[1 + slot]);
+            } else {
+                ARIEL_TRY(enqueue_step(s, s->ev[slot]));
+            }
+            s->ev_pending[slot] = true;
+            // read the previous step while this one runs
+            if (s->ev_pending[slot ^ 1]) ARIEL_TRY(collect_step_events(s, slot ^ 1));
+        } else {
+            if (s->prm.use_graph && !s->graph_tried[0]) try_build_graph(s, 0);
+            if (s->graph[0]) {
+                cudaError_t e = cudaGraphLaunch(s->graph[0], s->stream);
+                if (e != cudaSuccess) return map_cuda_error(e);
+                count_launch((int)s->graph_kernels[0]);
+            } else {
+                ARIEL_TRY(enqueue_step(s, nullptr));
+            }
+        }
+        for (auto& f : s->frames) f++;
+        if (s->prm.fail_on_not_converged) {
+            std::vector<PcgScene> sc(s->k);
+            ARIEL_CUDA(cudaMemcpyAsync(sc.data(), s->PA.sc, sizeof(PcgScene) * s->k, cudaMemcpyDeviceToHost, s->stream));
+            ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+            ARIEL_TRY(check_device_error(s));
+            for (auto& v : sc)
+                if (!v.converged) {
+                    s->last_status = ARIEL_ERR_NOT_CONVERGED;
+                    return ARIEL_ERR_NOT_CONVERGED;
+                }
+        }
+    }
+    if (timed) {
+        // the last step's events (its successor has not been launched)
+        for (int k2 = 0; k2 < 2; ++k2) {
+            int slot = s->ev_slot ^ 1 ^ k2;
+            if (s->ev_pending[slot]) ARIEL_TRY(collect_step_events(s, slot));
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return map_cuda_error(e);
+    return ARIEL_OK;
+}
+
+ariel_status ariel_synchronize(ariel_sim* s) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
+}
+
+ariel_status ariel_particle_count(ariel_sim* s, int32_t scene, int64_t* n) {
+    if (!s || !n || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    *n = s->ppref[scene + 1] - s->ppref[scene];
+    return ARIEL_OK;
+}
+
+ariel_status ariel_get_particles(ariel_sim* s, int32_t scene, float* pos, float* vel, float* density, float* mass,
+                                 int32_t* type) {
+    if (!s || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    const long long b = s->ppref[scene], n = s->ppref[scene + 1] - b;
+    if (n == 0) return ARIEL_OK;
+    std::vector<float4> p4(n), v4(n);
+    ARIEL_CUDA(copy_sync(s->stream, p4.data(), s->S.pos4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    ARIEL_CUDA(copy_sync(s->stream, v4.data(), s->S.vel4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    for (long long i = 0; i < n; ++i) {
+        if (pos) {
+            pos[3 * i] = p4[i].x;
+            pos[3 * i + 1] = p4[i].y;
+            pos[3 * i + 2] = p4[i].z;
+        }
+        if (vel) {
+            vel[3 * i] = v4[i].x;
+            vel[3 * i + 1] = v4[i].y;
+            vel[3 * i + 2] = v4[i].z;
+        }
+        if (mass) mass[i] = p4[i].w;
+        if (type) type[i] = type_bits(v4[i]);
+    }
+    if (density) {
+        cudaError_t e = launch_scatter_density(s->S, s->d_dens_id, s->stream);
+        if (e != cudaSuccess) return map_cuda_error(e);
+        ARIEL_CUDA(cudaMemcpyAsync(density, s->d_dens_id + b, n * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+        ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    return ARIEL_OK;
+}
+
+ariel_status ariel_get_cells(ariel_sim* s, int32_t scene, int32_t* particle_cell, int32_t* cell_count) {
+    if (!s || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    const long long pb = s->ppref[scene], pn = s->ppref[scene + 1] - pb;
+    const long long cb = s->cpref[scene], cn = s->cpref[scene + 1] - cb;
+    if (particle_cell && pn > 0) {
+        std::vector<uint32_t> key(pn);
+        ARIEL_CUDA(copy_sync(s->stream, key.data(), s->S.key + pb, pn * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        for (long long i = 0; i < pn; ++i) particle_cell[i] = (int32_t)((long long)key[i] - cb);
+    }
+    if (cell_count) ARIEL_CUDA(copy_sync(s->stream, cell_count, s->S.count + cb, cn * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return ARIEL_OK;
+}
+
+static ariel_status grid_span(ariel_sim* s, int32_t scene, int32_t which, void** dptr, size_t* elems, size_t* esize,
+                              bool* is_flags) {
+    const long long n = s->descs[scene].dim;
+    const long long per = n * n * (n + 1);
+    const long long fb = s->fpref[scene], cb = s->cpref[scene];
+    *is_flags = false;
+    switch (which) {
+        case ARIEL_GRID_UX: *dptr = s->S.u + fb; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_UY: *dptr = s->S.u + fb + per; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_UZ: *dptr = s->S.u + fb + 2 * per; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_PREV_UX: *dptr = s->S.pu + fb; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_PREV_UY: *dptr = s->S.pu + fb + per; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_PREV_UZ: *dptr = s->S.pu + fb + 2 * per; *elems = per; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_D: *dptr = s->S.D + cb; *elems = n * n * n; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_P: *dptr = s->S.P + cb; *elems = n * n * n; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_L: *dptr = s->S.L + cb; *elems = n * n * n; *esize = 4; return ARIEL_OK;
+        case ARIEL_GRID_A: *dptr = s->S.flags + cb; *elems = n * n * n; *esize = 4; *is_flags = true; return ARIEL_OK;
+        case ARIEL_GRID_P64: *dptr = s->S.P64 + cb; *elems = n * n * n; *esize = 8; return ARIEL_OK;
+    }
+    return ARIEL_ERR_INVALID_ARG;
+}
+
+ariel_status ariel_get_grid(ariel_sim* s, int32_t scene, int32_t which, void* buf, int64_t nbytes) {
+    if (!s || !buf || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    void* d;
+    size_t elems, esize;
+    bool flags;
+    ARIEL_TRY(grid_span(s, scene, which, &d, &elems, &esize, &flags));
+    if ((size_t)nbytes != elems * esize) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    if (flags) {
+        std::vector<uint8_t> f(elems);
+        ARIEL_CUDA(copy_sync(s->stream, f.data(), d, elems, cudaMemcpyDeviceToHost));
+        int32_t* o = (int32_t*)buf;
+        for (size_t i = 0; i < elems; ++i) o[i] = f[i];
+    } else {
+        ARIEL_CUDA(copy_sync(s->stream, buf, d, elems * esize, cudaMemcpyDeviceToHost));
+    }
+    return ARIEL_OK;
+}
+
+ariel_status ariel_set_grid(ariel_sim* s, int32_t scene, int32_t which, const void* buf, int64_t nbytes) {
+    if (!s || !buf || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    void* d;
+    size_t elems, esize;
+    bool flags;
+    ARIEL_TRY(grid_span(s, scene, which, &d, &elems, &esize, &flags));
+    if ((size_t)nbytes != elems * esize) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    if (flags) {
+        const int32_t* in = (const int32_t*)buf;
+        std::vector<uint8_t> f(elems);
+        for (size_t i = 0; i < elems; ++i) {
+            if (in[i] < 0 || in[i] > 2) return ARIEL_ERR_INVALID_ARG;
+            f[i] = (uint8_t)in[i];
+        }
+        ARIEL_CUDA(copy_sync(s->stream, d, f.data(), elems, cudaMemcpyHostToDevice));
+    } else {
+        ARIEL_CUDA(copy_sync(s->stream, d, buf, elems * esize, cudaMemcpyHostToDevice));
+    }
+    return ARIEL_OK;
+}
+
+ariel_status ariel_get_dimensions(ariel_sim* s, int32_t scene, int32_t* n) {
+    if (!s || !n || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    *n = s->descs[scene].dim;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_stats(ariel_sim* s, int32_t scene, AsimStats* out) {
+    if (!s || !out || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    PcgScene sc{};
+    ARIEL_CUDA(copy_sync(s->stream, &sc, s->PA.sc + scene, sizeof(PcgScene), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->frame = s->frames[scene];
+    out->n_particles = s->ppref[scene + 1] - s->ppref[scene];
+    out->n_fluid_cells = sc.nf;
+    out->pcg_iterations = sc.iters;
+    out->pcg_outer = s->mode == kMixed ? sc.outer : 1;
+    out->pcg_rr = sc.rr;
+    double rr = s->mode == kMixed ? sc.rr_out : sc.rr;
+    out->pcg_rel_residual = sc.bb > 0 ? std::sqrt(rr / sc.bb) : 0.0;
+    out->pcg_converged = sc.converged;
+    out->precond_exact_path = sc.ordered;
+    for (int g = 0; g < ARIEL_STAGE_COUNT; ++g) out->stage_ms[g] = s->stage_ms[g];
+    out->step_ms = s->step_ms;
+    out->last_status = s->last_status;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_get_max_density(ariel_sim* s, int32_t scene, float* md) {
+    if (!s || !md || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    *md = s->sh[scene].max_density;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_timer_begin(ariel_sim* s) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaEventRecord(s->tb, s->stream));
+    return ARIEL_OK;
+}
+
+ariel_status ariel_timer_end(ariel_sim* s, double* ms) {
+    if (!s || !ms) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaEventRecord(s->te, s->stream));
+    ARIEL_CUDA(cudaEventSynchronize(s->te));
+    float f = 0;
+    ARIEL_CUDA(cudaEventElapsedTime(&f, s->tb, s->te));
+    *ms = f;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_timing_reset(ariel_sim* s) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    for (int g = 0; g < ARIEL_STAGE_COUNT; ++g) s->acc_stage[g] = 0;
+    s->acc_solve_kernel = 0;
+    s->step_hist.clear();
+    ARIEL_CUDA(cudaMemsetAsync(s->PA.totals, 0, sizeof(PcgTotals) * s->k, s->stream));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return ARIEL_OK;
+}
+
+ariel_status ariel_solver_totals(ariel_sim* s, int32_t scene, AsimSolverTotals* out) {
+    if (!s || !out || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    PcgTotals t{};
+    ARIEL_CUDA(copy_sync(s->stream, &t, s->PA.totals + scene, sizeof(PcgTotals), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->solves = t.solves;
+    out->iterations = t.iterations;
+    out->outer = t.outer;
+    out->cell_iterations = t.cell_iterations;
+    out->cell_outer = t.cell_outer;
+    out->not_converged = t.not_converged;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_timing_get(ariel_sim* s, double* ms, double* solve_kernel_ms, double* step_ms, int32_t max_steps,
+                              int32_t* nsteps) {
+    if (!s) return ARIEL_ERR_INVALID_ARG;
+    if (ms)
+        for (int g = 0; g < ARIEL_STAGE_COUNT; ++g) ms[g] = s->acc_stage[g];
+    if (solve_kernel_ms) *solve_kernel_ms = s->acc_solve_kernel;
+    int n = (int)s->step_hist.size();
+    if (step_ms && max_steps > 0) {
+        int m = std::min(n, (int)max_steps);
+        for (int i = 0; i < m; ++i) step_ms[i] = s->step_hist[n - m + i];
+    }
+    if (nsteps) *nsteps = n;
+    return ARIEL_OK;
+}
+
+ariel_status ariel_upload_state(ariel_sim* s, int32_t scene, const float* pos, const float* vel) {
+    if (!s || !pos || !vel || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    const long long b = s->ppref[scene], n = s->ppref[scene + 1] - b;
+    if (n == 0) return ARIEL_OK;
+    float* sp = s->d_stage;
+    float* sv = s->d_stage + 3 * n;
+    ARIEL_CUDA(cudaMemcpyAsync(sp, pos, 12 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    ARIEL_CUDA(cudaMemcpyAsync(sv, vel, 12 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    ARIEL_CUDA(launch_unpack_state(s->S.pos4 + b, s->S.vel4 + b, sp, sv, n, s->S.dev_error, s->stream));
+    return ARIEL_OK;
+}
+
+ariel_status ariel_download_state(ariel_sim* s, int32_t scene, float* pos, float* vel) {
+    if (!s || !pos || !vel || scene < 0 || scene >= s->k) return ARIEL_ERR_INVALID_ARG;
+    const long long b = s->ppref[scene], n = s->ppref[scene + 1] - b;
+    if (n > 0) {
+        float* sp = s->d_stage;
+        float* sv = s->d_stage + 3 * n;
+        ARIEL_CUDA(launch_pack_state(s->S.pos4 + b, s->S.vel4 + b, sp, sv, n, s->stream));
+        ARIEL_CUDA(cudaMemcpyAsync(pos, sp, 12 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+        ARIEL_CUDA(cudaMemcpyAsync(vel, sv, 12 * (size_t)n, cudaMemcpyDeviceToHost, s->stream));
+    }
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
+}
+
+ariel_status ariel_selftest_barrier_timeout(double timeout_ms) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return ARIEL_ERR_NO_DEVICE;
+    }
+    Barrier* bar = nullptr;
+    int* err = nullptr;
+    ARIEL_CUDA(cudaMalloc(&bar, sizeof(Barrier)));
+    if (cudaMalloc(&err, sizeof(int)) != cudaSuccess) {
+        cudaFree(bar);
+        return ARIEL_ERR_OOM;
+    }
+    cudaMemset(err, 0, sizeof(int));
+    cudaError_t e = launch_barrier_selftest(bar, err, (unsigned long long)(timeout_ms * 1.0e6), 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int h = 0;
+    if (e == cudaSuccess) e = copy_sync(0, &h, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(bar);
+    cudaFree(err);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    return h ? ARIEL_ERR_DEVICE_TIMEOUT : ARIEL_OK;
+}
+
+int64_t ariel_kernel_launches(void) { return launch_count(); }
+
+const char* ariel_last_error(void) { return g_last_error; }
+
+}  // extern "C"

@@ -1,0 +1,694 @@
+// particles.cu -- particle-side stages of FlipSim::Step on sm_100a:
+//   sort-by-cell (ParticleGrid::Sort), ComputeDensity, ApplyExternalForces,
+//   SplatParticlesToMACGrid (deterministic per-face gather), SolvePicFlip + AdvectParticles,
+//   ResampleParticles, and the analytic-sphere solid constraints.
+//
+// Determinism: every sum runs in the reference's order -- neighbour cells sx -> sy -> sz
+// ascending, particles inside a cell in ascending particle id (the order ParticleGrid::Sort
+// appends them, particlegrid.cpp:150-171).  The cell sort therefore finishes each cell's
+// segment with an insertion sort by id after the arrival-order scatter.
+#include "state.cuh"
+
+namespace ariel {
+
+namespace {
+
+#define SCENE_PREFIX(pref_src)                       \
+    __shared__ long long pref_s[kMaxScenes + 1];     \
+    load_prefix<kMaxScenes>(pref_s, (pref_src), S.k)
+
+// ------------------------------------------------------------------------------------------
+// Analytic spheres (replaces Scene::IntersectSolidGeoms scene.cpp:425-434,
+// CheckPointInsideSolidGeom scene.cpp:382-402, LevelSet::ProjectPointsToSurface
+// levelset.cpp:175-193).  World (grid) units.
+// ------------------------------------------------------------------------------------------
+struct Hit {
+    bool hit;
+    float3 point, normal;
+};
+
+__device__ bool inside_solid(const SceneDev& D, float3 p) {
+    for (int i = 0; i < D.n_spheres; ++i) {
+        float4 s = D.sphere[i];
+        float3 d = f3sub(p, make_float3(s.x, s.y, s.z));
+        if (gdot3(d, d) < s.w * s.w) return true;
+    }
+    return false;
+}
+
+__device__ Hit intersect_solids(const SceneDev& D, float3 o, float3 dir) {
+    Hit best{false, make_float3(0, 0, 0), make_float3(0, 0, 0)};
+    float bestd = 0.0f;
+    for (int i = 0; i < D.n_spheres; ++i) {
+        float4 s = D.sphere[i];
+        float3 c = make_float3(s.x, s.y, s.z);
+        float3 oc = f3sub(o, c);
+        float b = gdot3(dir, oc);
+        float cc = gdot3(oc, oc) - s.w * s.w;
+        float disc = b * b - cc;
+        if (!(disc >= 0.0f)) continue;
+        float sq = sqrtf(disc);
+        float t = -b - sq;
+        if (!(t > 0.0f)) t = -b + sq;
+        if (!(t > 0.0f)) continue;
+        float3 pt = f3add(o, f3mul(dir, t));
+        float3 nrm = gnormalize3(f3sub(pt, c));
+        float d = glength3(f3sub(pt, o));
+        if (!best.hit || !(bestd <= d)) {
+            best.hit = true;
+            best.point = pt;
+            best.normal = nrm;
+            bestd = d;
+        }
+    }
+    return best;
+}
+
+__device__ float3 closest_solid_surface(const SceneDev& D, float3 p) {
+    for (int i = 0; i < D.n_spheres; ++i) {
+        float4 s = D.sphere[i];
+        float3 c = make_float3(s.x, s.y, s.z);
+        float3 d = f3sub(p, c);
+        if (gdot3(d, d) < s.w * s.w) return f3add(c, f3mul(gnormalize3(d), s.w));
+    }
+    return p;
+}
+
+// FlipSim::CheckParticleSolidConstraints for one FLUID particle (flip.cpp:183-227).
+__device__ void solid_constraints(const SceneDev& D, float3& p, float3& u, float3 pt, float3 ut) {
+    const float maxd = D.maxd;
+    float3 origin = f3mul(pt, maxd);
+    float3 dir = gnormalize3(f3sub(p, pt));
+    float raynulltest = glength3(dir);
+    if (!(raynulltest == raynulltest)) return;
+    Hit hit = intersect_solids(D, origin, dir);
+    float u_dir = glength3(ut);
+    if (hit.hit) {
+        float solidDistance = glength3(f3sub(origin, hit.point));
+        float velocityDistance = glength3(f3sub(p, pt)) * maxd;
+        if (solidDistance < velocityDistance) {
+            p = f3div(f3add(origin, f3mul(f3mul(dir, .90f), solidDistance)), maxd);
+            float3 r = f3sub(f3smul(2.0f * gdot3(dir, hit.normal), hit.normal), gnormalize3(dir));
+            u = f3mul(gnormalize3(r), u_dir);
+        }
+    }
+    float3 o2 = f3mul(p, maxd);
+    if (inside_solid(D, o2)) {
+        float3 nd = gnormalize3(dir);
+        u = f3mul(make_float3(-nd.x, -nd.y, -nd.z), u_dir);
+        p = f3add(pt, f3mul(u, D.dt));
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// BEGIN: frame++, AdjustParticlesStuckInSolids (flip.cpp:130-181), StoreTemp (flip.cpp:79-90)
+// ------------------------------------------------------------------------------------------
+__global__ void k_frame_inc(SceneDev* scenes, int k) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < k) scenes[s].frame += 1;
+}
+
+__global__ void k_begin_solids(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.np) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
+    float4 p4 = S.pos4[g];
+    float4 v4 = S.vel4[g];
+    if (D.n_spheres > 0 && type_of(v4) == ARIEL_FLUID) {
+        const float maxd = D.maxd;
+        float3 p = make_float3(p4.x, p4.y, p4.z);
+        if (inside_solid(D, f3mul(p, maxd))) {
+            float3 pt = p;
+            float3 np = f3div(closest_solid_surface(D, f3mul(p, maxd)), maxd);
+            float3 origin = f3mul(pt, maxd);
+            float3 dir = gnormalize3(f3sub(np, pt));
+            float d = glength3(f3sub(np, pt));
+            float raynulltest = glength3(dir);
+            p = np;
+            if (raynulltest == raynulltest) {
+                Hit hit = intersect_solids(D, origin, dir);
+                float nearest = glength3(f3sub(origin, hit.point));
+                p = f3div(f3add(origin, f3mul(f3mul(dir, 1.05f), nearest)), maxd);
+                float3 u = f3mul(gnormalize3(dir), d);
+                v4.x = u.x;
+                v4.y = u.y;
+                v4.z = u.z;
+            }
+            p4.x = p.x;
+            p4.y = p.y;
+            p4.z = p.z;
+            S.pos4[g] = p4;
+            S.vel4[g] = v4;
+        }
+    }
+    S.pt4[g] = p4;
+    S.ut4[g] = v4;
+}
+
+// ------------------------------------------------------------------------------------------
+// Sort-by-cell (replaces ParticleGrid::Sort, particlegrid.cpp:140-172)
+// ------------------------------------------------------------------------------------------
+__global__ void k_sort_key(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.np) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
+    float4 p = S.pos4[g];
+    const int n = D.n;
+    int ci = cell_coord(D.maxd, p.x), cj = cell_coord(D.maxd, p.y), ck = cell_coord(D.maxd, p.z);
+    uint32_t c = (uint32_t)(D.c_begin + ((long long)ci * n + cj) * n + ck);
+    S.key[g] = c;
+    S.off[g] = atomicAdd(&S.count[c], 1u);
+}
+
+__global__ void k_sort_scatter(DevState S) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.np) return;
+    uint32_t c = S.key[g];
+    S.sid[S.start[c] + S.off[g]] = (uint32_t)g;
+}
+
+// Restores ascending particle id inside each cell (the reference's append order).
+__global__ void k_sort_cells(DevState S) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= S.nc) return;
+    uint32_t a = S.start[c], b = S.start[c + 1];
+    if (b - a < 2) return;
+    uint32_t* seg = S.sid + a;
+    uint32_t m = b - a;
+    for (uint32_t i = 1; i < m; ++i) {
+        uint32_t v = seg[i];
+        uint32_t j = i;
+        while (j > 0 && seg[j - 1] > v) {
+            seg[j] = seg[j - 1];
+            --j;
+        }
+        seg[j] = v;
+    }
+}
+
+__global__ void k_sort_permute(DevState S) {
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.np) return;
+    uint32_t g = S.sid[s];
+    S.spos4[s] = S.pos4[g];
+    S.svel4[s] = S.vel4[g];
+}
+
+// ------------------------------------------------------------------------------------------
+// FlipSim::ComputeDensity (flip.cpp:697-733): one thread per slot, 27-cell gather.
+// ------------------------------------------------------------------------------------------
+__global__ void k_density(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.np) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, s)];
+    float4 p = S.spos4[s];
+    if (type_of(S.svel4[s]) == ARIEL_SOLID) {
+        S.dens[s] = 1.0f;
+        return;
+    }
+    const int n = D.n;
+    const float hk = D.dens_h;
+    int ci = cell_coord(D.maxd, p.x), cj = cell_coord(D.maxd, p.y), ck = cell_coord(D.maxd, p.z);
+    int z0 = max(ck - 1, 0), z1 = min(ck + 1, n - 1);
+    float weightsum = 0.0f;
+    for (int sx = ci - 1; sx <= ci + 1; ++sx) {
+        if (sx < 0 || sx > n - 1) continue;
+        for (int sy = cj - 1; sy <= cj + 1; ++sy) {
+            if (sy < 0 || sy > n - 1) continue;
+            long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+            uint32_t a = S.start[cb + z0], b = S.start[cb + z1 + 1];
+            for (uint32_t t = a; t < b; ++t) {
+                float4 q = S.spos4[t];
+                float sqd = sqrlength(q.x, q.y, q.z, p.x, p.y, p.z);
+                float weight = q.w * smooth_k(sqd, hk);
+                weightsum = weightsum + weight;
+            }
+        }
+    }
+    S.dens[s] = weightsum / D.max_density;
+}
+
+__global__ void k_fill_dens(DevState S, float v) {
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S.np) S.dens[s] = v;
+}
+
+__global__ void k_scatter_density(DevState S, float* out) {
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S.np) out[S.sid[s]] = S.dens[s];
+}
+
+// ------------------------------------------------------------------------------------------
+// FlipSim::ApplyExternalForces (flip.cpp:682-695): on the slot copy and the id-order state.
+// ------------------------------------------------------------------------------------------
+__global__ void k_forces(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.np) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, s)];
+    float4 v = S.svel4[s];
+    for (int j = 0; j < D.n_forces; ++j) {
+        v.x = v.x + D.fdt[j][0];
+        v.y = v.y + D.fdt[j][1];
+        v.z = v.z + D.fdt[j][2];
+    }
+    S.svel4[s] = v;
+    S.vel4[S.sid[s]] = v;
+}
+
+// ------------------------------------------------------------------------------------------
+// SplatParticlesToMACGrid (particlegridoperations.inl:146-249): every face gathers the FLUID
+// particles of its 2x4x4 cell block (GetWallNeighbors, particlegrid.cpp:52-73) with the
+// Sharpen kernel of radius 1.4 cells.  Face-parallel, so no atomics and a fixed order.
+// ------------------------------------------------------------------------------------------
+__global__ void k_p2g(DevState S) {
+    SCENE_PREFIX(S.f_pref);
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.nf) return;
+    int sc = find_scene(pref_s, S.k, g);
+    const SceneDev& D = S.scenes[sc];
+    const int n = D.n;
+    const long long per = (long long)n * n * (n + 1);
+    long long f = g - D.f_begin;
+    int axis = (int)(f / per);
+    long long rem = f - axis * per;
+    int i, j, k;
+    if (axis == 0) {
+        i = (int)(rem / ((long long)n * n));
+        j = (int)((rem / n) % n);
+        k = (int)(rem % n);
+    } else if (axis == 1) {
+        i = (int)(rem / ((long long)(n + 1) * n));
+        j = (int)((rem / n) % (n + 1));
+        k = (int)(rem % n);
+    } else {
+        i = (int)(rem / ((long long)n * (n + 1)));
+        j = (int)((rem / (n + 1)) % n);
+        k = (int)(rem % (n + 1));
+    }
+    // face centre and GetWallNeighbors block [index - nn, index + nn - 1]
+    float fx, fy, fz;
+    int xlo, xhi, ylo, yhi, zlo, zhi;
+    if (axis == 0) {
+        fx = (float)i; fy = j + 0.5f; fz = k + 0.5f;
+        xlo = i - 1; xhi = i; ylo = j - 2; yhi = j + 1; zlo = k - 2; zhi = k + 1;
+    } else if (axis == 1) {
+        fx = i + 0.5f; fy = (float)j; fz = k + 0.5f;
+        xlo = i - 2; xhi = i + 1; ylo = j - 1; yhi = j; zlo = k - 2; zhi = k + 1;
+    } else {
+        fx = i + 0.5f; fy = j + 0.5f; fz = (float)k;
+        xlo = i - 2; xhi = i + 1; ylo = j - 2; yhi = j + 1; zlo = k - 1; zhi = k;
+    }
+    xlo = max(xlo, 0); xhi = min(xhi, n - 1);
+    ylo = max(ylo, 0); yhi = min(yhi, n - 1);
+    zlo = max(zlo, 0); zhi = min(zhi, n - 1);
+    const float RE = 1.4f;
+    const float RE2 = RE * RE;
+    const float maxd = D.maxd;
+    float sumw = 0.0f, sumu = 0.0f;
+    if (zlo <= zhi) {
+        for (int sx = xlo; sx <= xhi; ++sx) {
+            for (int sy = ylo; sy <= yhi; ++sy) {
+                long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                uint32_t a = S.start[cb + zlo], b = S.start[cb + zhi + 1];
+                for (uint32_t t = a; t < b; ++t) {
+                    float4 v = S.svel4[t];
+                    if (type_of(v) != ARIEL_FLUID) continue;
+                    float4 q = S.spos4[t];
+                    float px = gmax(0.0f, gmin(maxd, maxd * q.x));
+                    float py = gmax(0.0f, gmin(maxd, maxd * q.y));
+                    float pz = gmax(0.0f, gmin(maxd, maxd * q.z));
+                    float r2 = sqrlength(px, py, pz, fx, fy, fz);
+                    // Sharpen is exactly 0 for r2 >= RE^2, so such particles add nothing.
+                    if (!(r2 < RE2)) continue;
+                    float w = q.w * sharpen_k(r2, RE);
+                    float uc = axis == 0 ? v.x : (axis == 1 ? v.y : v.z);
+                    sumu += w * uc;
+                    sumw += w;
+                }
+            }
+        }
+    }
+    float val = 0.0f;
+    if (sumw > 0) val = sumu / sumw;
+    S.u[g] = val;
+}
+
+// ------------------------------------------------------------------------------------------
+// Interpolate / InterpolateVelocity (particlegridoperations.inl:106-133)
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ float interp1(const float* __restrict__ q, int ey, int ez, float px, float py, float pz,
+                                         float nx, float ny, float nz) {
+    float x = gmax(0.0f, gmin(nx, px));
+    float y = gmax(0.0f, gmin(ny, py));
+    float z = gmax(0.0f, gmin(nz, pz));
+    int i = (int)gmin(x, nx - 2);
+    int j = (int)gmin(y, ny - 2);
+    int k = (int)gmin(z, nz - 2);
+    auto Q = [&](int a, int b, int c) { return q[((long long)a * ey + b) * ez + c]; };
+    float fi1 = (float)(i + 1), fj1 = (float)(j + 1), fk1 = (float)(k + 1);
+    float term1 = ((fi1 - x) * Q(i, j, k) + (x - i) * Q(i + 1, j, k)) * (fj1 - y);
+    float term2 = ((fi1 - x) * Q(i, j + 1, k) + (x - i) * Q(i + 1, j + 1, k)) * (y - j);
+    float term3 = ((fi1 - x) * Q(i, j, k + 1) + (x - i) * Q(i + 1, j, k + 1)) * (fj1 - y);
+    float term4 = ((fi1 - x) * Q(i, j + 1, k + 1) + (x - i) * Q(i + 1, j + 1, k + 1)) * (y - j);
+    return (fk1 - z) * (term1 + term2) + (z - k) * (term3 + term4);
+}
+
+__device__ __forceinline__ float3 interp_vel(const float* __restrict__ faces, int n, float3 p) {
+    const long long per = (long long)n * n * (n + 1);
+    const float X = (float)n;
+    float3 u;
+    u.x = interp1(faces, n, n, X * p.x, X * p.y - 0.5f, X * p.z - 0.5f, (float)(n + 1), X, X);
+    u.y = interp1(faces + per, n + 1, n, X * p.x - 0.5f, X * p.y, X * p.z - 0.5f, X, (float)(n + 1), X);
+    u.z = interp1(faces + 2 * per, n, n + 1, X * p.x - 0.5f, X * p.y - 0.5f, X * p.z, X, X, (float)(n + 1));
+    return u;
+}
+
+// ------------------------------------------------------------------------------------------
+// SolvePicFlip (flip.cpp:287-322) + AdvectParticles (flip.cpp:229-285) +
+// CheckParticleSolidConstraints (flip.cpp:183-227), one thread per particle (id order).
+// ------------------------------------------------------------------------------------------
+__global__ void k_g2p_advect(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= S.np) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
+    const int n = D.n;
+    float4 p4 = S.pos4[g];
+    float4 v4 = S.vel4[g];
+    const float* cur = S.u + D.f_begin;
+    const float* prv = S.pu + D.f_begin;
+    float3 p = make_float3(p4.x, p4.y, p4.z);
+    float3 t = make_float3(v4.x, v4.y, v4.z);
+    float3 du = interp_vel(prv, n, p);
+    t = f3add(du, t);
+    float3 pic = interp_vel(cur, n, p);
+    const float pf = D.picflip;
+    const float opf = 1.0f - pf;
+    float3 u = f3add(f3smul(opf, pic), f3smul(pf, t));
+    if (type_of(v4) == ARIEL_FLUID) {
+        p = f3add(p, f3smul(D.dt, pic));
+        const float r = 1.0f / D.maxd;
+        p.x = gmax(r, gmin(1.0f - r, p.x));
+        p.y = gmax(r, gmin(1.0f - r, p.y));
+        p.z = gmax(r, gmin(1.0f - r, p.z));
+        if (D.n_spheres > 0) {
+            // solid push-out against the static SOLID particles of the 27 cells
+            const float maxd = D.maxd;
+            unsigned ci = (unsigned)gmin((float)n - 1.0f, p.x * maxd);
+            unsigned cj = (unsigned)gmin((float)n - 1.0f, p.y * maxd);
+            unsigned ck = (unsigned)gmin((float)n - 1.0f, p.z * maxd);
+            const float re = D.pushout_re;
+            int z0 = max((int)ck - 1, 0), z1 = min((int)ck + 1, n - 1);
+            for (int sx = (int)ci - 1; sx <= (int)ci + 1; ++sx) {
+                if (sx < 0 || sx > n - 1) continue;
+                for (int sy = (int)cj - 1; sy <= (int)cj + 1; ++sy) {
+                    if (sy < 0 || sy > n - 1) continue;
+                    long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                    uint32_t a = S.solid_start[cb + z0], b = S.solid_start[cb + z1 + 1];
+                    for (uint32_t q = a; q < b; ++q) {
+                        float4 sp = S.solid_pos[q];
+                        float3 d = f3sub(p, make_float3(sp.x, sp.y, sp.z));
+                        float dist = glength3(d);
+                        if (dist < re) {
+                            float3 normal = make_float3(0, 0, 0);
+                            if (glength3(normal) < 0.0000001f && dist != 0.0f) normal = gnormalize3(d);
+                            p = f3add(p, f3smul(re - dist, normal));
+                            u = f3sub(u, f3smul(gdot3(u, normal), normal));
+                        }
+                    }
+                }
+            }
+            float4 pt = S.pt4[g], ut = S.ut4[g];
+            solid_constraints(D, p, u, make_float3(pt.x, pt.y, pt.z), make_float3(ut.x, ut.y, ut.z));
+        }
+    }
+    S.pos4[g] = make_float4(p.x, p.y, p.z, p4.w);
+    S.vel4[g] = make_float4(u.x, u.y, u.z, v4.w);
+}
+
+// ------------------------------------------------------------------------------------------
+// ResampleParticles + Resample (particleresampler.inl:35-148) + CheckParticleSolidConstraints,
+// one thread per slot of the resampler's own Sort.  rand() becomes Philox keyed by
+// (rng seed, frame, particle id, draw ordinal).
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void nb_range(float x, int n, int& lo, int& hi) {
+    // GetCellNeighbors with a fractional index and radius 1 (particlegrid.cpp:32-35)
+    lo = (int)(x - 1.0f);
+    hi = (int)floorf(x + 1.0f);
+    if (lo < 0) lo = 0;
+    if (hi > n - 1) hi = n - 1;
+}
+
+__global__ void k_resample(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.np) return;
+    float4 p4 = S.spos4[s];
+    float4 v4 = S.svel4[s];
+    if (type_of(v4) != ARIEL_FLUID) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, s)];
+    if (D.resample_every <= 0 || D.frame % D.resample_every != 0) return;
+    const int n = D.n;
+    const float maxd = D.maxd;
+    const float dt = D.dt;
+    const float re = D.resample_re;
+    const float springforce = 50.0f;
+    const float re2 = re * re;
+    const uint32_t g = S.sid[s];
+    const uint32_t gid = (uint32_t)(g - D.p_begin);
+    const uint32_t k0 = (uint32_t)D.rng_seed, k1 = (uint32_t)(D.rng_seed >> 32);
+    float3 spring = make_float3(0, 0, 0);
+    {
+        float x = gmax(0.0f, gmin(maxd, maxd * p4.x));
+        float y = gmax(0.0f, gmin(maxd, maxd * p4.y));
+        float z = gmax(0.0f, gmin(maxd, maxd * p4.z));
+        int xl, xh, yl, yh, zl, zh;
+        nb_range(x, n, xl, xh);
+        nb_range(y, n, yl, yh);
+        nb_range(z, n, zl, zh);
+        uint32_t draws = 0;
+        if (zl <= zh) {
+            for (int sx = xl; sx <= xh; ++sx)
+                for (int sy = yl; sy <= yh; ++sy) {
+                    long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                    uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                    for (uint32_t t = a; t < b; ++t) {
+                        if (t == (uint32_t)s) continue;
+                        float4 q = S.spos4[t];
+                        float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
+                        float dd = gdot3(d, d);
+                        // Beyond twice re^2 the Smooth weight is exactly 0 and the jitter branch
+                        // (dist <= 0.1 re) cannot trigger, so the neighbour adds exactly nothing.
+                        if (!(dd < 2.0f * re2)) continue;
+                        float dist = sqrtf(dd);
+                        if (!(dist * dist < re2) && dist > 0.1f * re) continue;  // w == 0 exactly
+                        float w = springforce * q.w * smooth_k(dist * dist, re);
+                        if (dist > 0.1f * re) {
+                            spring.x += w * (p4.x - q.x) / dist * re;
+                            spring.y += w * (p4.y - q.y) / dist * re;
+                            spring.z += w * (p4.z - q.z) / dist * re;
+                        } else if (type_of(S.svel4[t]) == ARIEL_FLUID) {
+                            uint4 rv = philox4x32_10(make_uint4(gid, (uint32_t)D.frame, draws++, kTagResample), k0, k1);
+                            spring.x += 0.01f * re / dt * (float)(rv.x % 101u) / 100.0f;
+                            spring.y += 0.01f * re / dt * (float)(rv.y % 101u) / 100.0f;
+                            spring.z += 0.01f * re / dt * (float)(rv.z % 101u) / 100.0f;
+                        } else {
+                            // SOLID neighbour: its normal m_n is zero for scene-generated solids
+                            spring.x += 0.05f * re / dt * 0.0f;
+                            spring.y += 0.05f * re / dt * 0.0f;
+                            spring.z += 0.05f * re / dt * 0.0f;
+                        }
+                    }
+                }
+        }
+    }
+    float3 t;
+    t.x = p4.x + dt * spring.x;
+    t.y = p4.y + dt * spring.y;
+    t.z = p4.z + dt * spring.z;
+    // Resample (particleresampler.inl:120-148)
+    float wsum = 0.0f;
+    float3 ru = make_float3(0, 0, 0);
+    {
+        float x = gmax(0.0f, gmin(maxd - 1, maxd * t.x));
+        float y = gmax(0.0f, gmin(maxd - 1, maxd * t.y));
+        float z = gmax(0.0f, gmin(maxd - 1, maxd * t.z));
+        int xl, xh, yl, yh, zl, zh;
+        nb_range(x, n, xl, xh);
+        nb_range(y, n, yl, yh);
+        nb_range(z, n, zl, zh);
+        if (zl <= zh) {
+            for (int sx = xl; sx <= xh; ++sx)
+                for (int sy = yl; sy <= yh; ++sy) {
+                    long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                    uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                    for (uint32_t q = a; q < b; ++q) {
+                        float4 np = S.spos4[q];
+                        float dist2 = sqrlength(t.x, t.y, t.z, np.x, np.y, np.z);
+                        // Sharpen is exactly 0 for dist2 >= re^2
+                        if (!(dist2 < re2)) continue;
+                        float4 nv = S.svel4[q];
+                        if (type_of(nv) != ARIEL_FLUID) continue;
+                        float w = np.w * sharpen_k(dist2, re);
+                        ru.x = ru.x + w * nv.x;
+                        ru.y = ru.y + w * nv.y;
+                        ru.z = ru.z + w * nv.z;
+                        wsum += w;
+                    }
+                }
+        }
+    }
+    if (wsum != 0.0f)
+        ru = f3div(ru, wsum);
+    else
+        ru = make_float3(v4.x, v4.y, v4.z);
+    float3 p = make_float3(p4.x, p4.y, p4.z);
+    float3 u = make_float3(v4.x, v4.y, v4.z);
+    if (!(D.n_spheres > 0 && inside_solid(D, f3mul(t, maxd)))) {
+        p = t;
+        u = ru;
+    }
+    if (D.n_spheres > 0)
+        solid_constraints(D, p, u, make_float3(p4.x, p4.y, p4.z), make_float3(v4.x, v4.y, v4.z));
+    S.pos4[g] = make_float4(p.x, p.y, p.z, p4.w);
+    S.vel4[g] = make_float4(u.x, u.y, u.z, v4.w);
+}
+
+__global__ void k_unpack_state(float4* pos4, float4* vel4, const float* __restrict__ pos,
+                               const float* __restrict__ vel, long long n, int* err) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos4[i], v = vel4[i];
+    p.x = pos[3 * i];
+    p.y = pos[3 * i + 1];
+    p.z = pos[3 * i + 2];
+    v.x = vel[3 * i];
+    v.y = vel[3 * i + 1];
+    v.z = vel[3 * i + 2];
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
+        atomicOr(err, 2);
+    pos4[i] = p;
+    vel4[i] = v;
+}
+
+__global__ void k_pack_state(const float4* __restrict__ pos4, const float4* __restrict__ vel4, float* pos, float* vel,
+                             long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos4[i], v = vel4[i];
+    pos[3 * i] = p.x;
+    pos[3 * i + 1] = p.y;
+    pos[3 * i + 2] = p.z;
+    vel[3 * i] = v.x;
+    vel[3 * i + 1] = v.y;
+    vel[3 * i + 2] = v.z;
+}
+
+}  // namespace
+
+cudaError_t launch_unpack_state(float4* pos4, float4* vel4, const float* pos, const float* vel, long long n,
+                                int* err, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_unpack_state<<<grid_for(n), kBlock, 0, st>>>(pos4, vel4, pos, vel, n, err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_state(const float4* pos4, const float4* vel4, float* pos, float* vel, long long n,
+                              cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_pack_state<<<grid_for(n), kBlock, 0, st>>>(pos4, vel4, pos, vel, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------------------------
+cudaError_t launch_begin(const DevState& S, cudaStream_t st) {
+    k_frame_inc<<<grid_for(S.k), kBlock, 0, st>>>(const_cast<SceneDev*>(S.scenes), S.k);
+    count_launch();
+    if (S.any_solid && S.np > 0) {
+        k_begin_solids<<<grid_for(S.np), kBlock, 0, st>>>(S);
+        count_launch();
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t sort_core(const DevState& S, void* scan_tmp, cudaStream_t st) {
+    cudaMemsetAsync(S.count, 0, sizeof(uint32_t) * (size_t)S.nc, st);
+    if (S.np > 0) {
+        k_sort_key<<<grid_for(S.np), kBlock, 0, st>>>(S);
+        count_launch();
+    }
+    cudaError_t e = launch_scan_u32(S.count, S.start, S.nc, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    if (S.np > 0) {
+        k_sort_scatter<<<grid_for(S.np), kBlock, 0, st>>>(S);
+        k_sort_cells<<<grid_for(S.nc), kBlock, 0, st>>>(S);
+        k_sort_permute<<<grid_for(S.np), kBlock, 0, st>>>(S);
+        count_launch(3);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort(const DevState& S, void* scan_tmp, cudaStream_t st) { return sort_core(S, scan_tmp, st); }
+
+cudaError_t launch_density(const DevState& S, cudaStream_t st) {
+    if (S.np == 0) return cudaSuccess;
+    k_density<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill_dens(const DevState& S, float value, cudaStream_t st) {
+    if (S.np == 0) return cudaSuccess;
+    k_fill_dens<<<grid_for(S.np), kBlock, 0, st>>>(S, value);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_density(const DevState& S, float* out, cudaStream_t st) {
+    if (S.np == 0) return cudaSuccess;
+    k_scatter_density<<<grid_for(S.np), kBlock, 0, st>>>(S, out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forces(const DevState& S, cudaStream_t st) {
+    if (S.np == 0) return cudaSuccess;
+    k_forces<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_p2g(const DevState& S, cudaStream_t st) {
+    if (S.nf == 0) return cudaSuccess;
+    k_p2g<<<grid_for(S.nf), kBlock, 0, st>>>(S);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_g2p_advect(const DevState& S, cudaStream_t st) {
+    if (S.np == 0) return cudaSuccess;
+    k_g2p_advect<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resample(const DevState& S, void* scan_tmp, cudaStream_t st) {
+    // StoreTempParticleVelocities before the resampler (flip.cpp:119) needs no copy: the
+    // resampler's constraint check reads pt/ut from the slot copies of its own Sort.
+    cudaError_t e = sort_core(S, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    if (S.np == 0) return cudaSuccess;
+    k_resample<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace ariel

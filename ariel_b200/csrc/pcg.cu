@@ -1,0 +1,976 @@
+// pcg.cu -- the pressure Poisson solve (Solve, src/sim/solver.inl:356-379) on sm_100a.
+//
+// One cooperative, persistent kernel runs the whole solve for every scene of the handle:
+// FLUID cells are split into fixed-size chunks that belong to exactly one scene; each chunk
+// writes its partial dot products; the last block to arrive at a grid barrier reduces each
+// scene's chunk partials in a fixed order and updates that scene's alpha/beta/stop state.
+// Results therefore do not depend on block scheduling, nor on which other scenes share the
+// launch (a scene's chunk boundaries depend only on its own FLUID count).
+//
+// Precision modes:
+//   kRef32 -- the reference's fp32 arithmetic: ComputeAx's exact expression (solver.inl:196-230),
+//             Op's x + alpha*y updates (:157-177), fp32 alpha/beta; dots accumulate in fp64 and
+//             are rounded to fp32 (the reference's serial float Product is only less accurate).
+//   kFp64  -- every vector and scalar fp64 (the plain FP64 GPU path).
+//   kMixed -- fp64 iterative refinement: true residual, x and dots in fp64; each correction
+//             solve's SpMV, preconditioner apply and vector updates in fp32.
+// Preconditioner: the reference's (elementwise unless a FLUID value is exactly 1.0, then an
+// ordered i+j+k hyperplane sweep), or MIC(0) (ordered sweeps).
+//
+// Every wait is bounded by a globaltimer budget; on expiry the kernel records an error word
+// and all blocks return.
+#include <cooperative_groups.h>
+
+#include "pcg.cuh"
+
+namespace ariel {
+
+namespace {
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier for co-resident blocks.  The last block to arrive runs `leader` (all of its
+// threads) before releasing the others.  Returns false if the wait ran out of time or another
+// block reported an error; the caller must then return.
+template <class F>
+__device__ bool grid_barrier(Barrier* bar, int* dev_error, unsigned long long timeout_ns, F&& leader) {
+    __shared__ int s_last, s_ok;
+    __shared__ unsigned s_gen;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned g = ld_acquire_u32(&bar->gen);
+        s_gen = g;
+        __threadfence();
+        unsigned arrived = atomicAdd(&bar->count, 1u);
+        s_last = (arrived == gridDim.x - 1);
+        s_ok = 1;
+        if (!s_last) {
+            unsigned long long t0 = gtimer();
+            while (ld_acquire_u32(&bar->gen) == g) {
+                if (*(volatile int*)&bar->error) {
+                    s_ok = 0;
+                    break;
+                }
+                if (gtimer() - t0 > timeout_ns) {
+                    atomicExch(&bar->error, 1);
+                    if (dev_error) atomicExch(dev_error, 1);
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    if (s_last) {
+        leader();
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            bar->count = 0;
+            __threadfence();
+            st_release_u32(&bar->gen, s_gen + 1);
+        }
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+struct NoLeader {
+    __device__ void operator()() const {}
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block reduction of two values; result valid in thread 0.
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+    __shared__ double sa[kPcgThreads / 32], sb[kPcgThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (lane == 0) {
+        sa[wid] = a;
+        sb[wid] = b;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        a = lane < kPcgThreads / 32 ? sa[lane] : 0.0;
+        b = lane < kPcgThreads / 32 ? sb[lane] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+    }
+    __syncthreads();
+}
+
+// Sum of partial[b..e) by one warp in a fixed tree that depends only on e-b (so a scene's
+// result does not depend on which scenes share the launch); valid in every lane.  Loads are
+// issued 16 per lane before any add so that the leader pays about one L2 round trip.
+__device__ __forceinline__ double scene_sum(const double* part, long long b, long long e) {
+    const int lane = threadIdx.x & 31;
+    double v = 0.0;
+    for (long long base = b; base < e; base += 32 * 16) {
+        double x[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            long long c = base + (long long)u * 32 + lane;
+            x[u] = c < e ? __ldcg(part + c) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) v += x[u];
+    }
+    v = warp_sum(v);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Whole-struct read of a scene's solver state through L2 (never a possibly stale L1 line).
+__device__ __forceinline__ PcgScene load_sc(const PcgScene* p) {
+    PcgScene v;
+    const int4* src = reinterpret_cast<const int4*>(p);
+    int4* dst = reinterpret_cast<int4*>(&v);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(PcgScene) / 16); ++i) dst[i] = __ldcg(src + i);
+    return v;
+}
+
+template <int MODE>
+struct VT {
+    using T = float;
+};
+template <>
+struct VT<kFp64> {
+    using T = double;
+};
+
+__device__ __forceinline__ void cell_ijk(long long local, int n, int& i, int& j, int& k) {
+    i = (int)(local / ((long long)n * n));
+    j = (int)((local / n) % n);
+    k = (int)(local % n);
+}
+
+// ------------------------------------------------------------------------------------------
+// Preparation: per-cell operator data, order-free preconditioner, FLUID predicate.
+// ------------------------------------------------------------------------------------------
+__global__ void k_prep_cells(PcgArgs A, uint32_t* pred) {
+    const DevState& S = A.S;
+    __shared__ long long pref_s[kMaxScenes + 1];
+    load_prefix<kMaxScenes>(pref_s, S.c_pref, S.k);
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= S.nc) return;
+    int s = find_scene(pref_s, S.k, c);
+    const SceneDev& D = S.scenes[s];
+    const int n = D.n;
+    const uint8_t flag = S.flags[c];
+    pred[c] = flag == ARIEL_FLUID;
+    if (flag != ARIEL_FLUID) {
+        S.P[c] = 0.0f;
+        if (S.P64) S.P64[c] = 0.0;
+        A.mask[c] = 0;
+        A.diag[c] = 0.0;
+        A.pc64[c] = 0.0;
+        A.pc32[c] = 0.0f;
+        return;
+    }
+    int i, j, k;
+    cell_ijk(c - D.c_begin, n, i, j, k);
+    const int q[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
+    const float Lc = S.L[c];
+    float d32 = 6.0f;
+    double d64 = 6.0;
+    uint8_t m = 0;
+    for (int d = 0; d < 6; ++d) {
+        int qi = q[d][0], qj = q[d][1], qk = q[d][2];
+        if (qi < 0 || qi > n - 1 || qj < 0 || qj > n - 1 || qk < 0 || qk > n - 1) {
+            d32 -= 1.0f;
+            d64 -= 1.0;
+            continue;
+        }
+        long long qc = D.c_begin + ((long long)qi * n + qj) * n + qk;
+        uint8_t tq = S.flags[qc];
+        if (tq == ARIEL_SOLID) {
+            d32 -= 1.0f;
+            d64 -= 1.0;
+        } else if (tq == ARIEL_FLUID) {
+            m |= (uint8_t)(1u << d);
+        } else if (D.subcell) {
+            // ADiag (solver.inl:95-96): diag -= L_q / min(1e-6, L_c)
+            d32 -= S.L[qc] / gmin(1.0e-6f, Lc);
+            d64 -= (double)S.L[qc] / (double)gmin(1.0e-6f, Lc);
+        }
+    }
+    A.mask[c] = m;
+    int one = 0;
+    if (A.mode == kRef32) {
+        // BuildPreconditioner (solver.inl:113-128) with its neighbour terms zero
+        float e = d32 - (0.0f * 0.0f) - (0.0f * 0.0f) - (0.0f * 0.0f);
+        float pc = 0.0f;
+        if (d32 > 0) {
+            if (e < 0.25f * d32) e = d32;
+            pc = 1.0f / sqrtf(e);
+        }
+        A.diag[c] = (double)d32;
+        A.pc32[c] = pc;
+        A.pc64[c] = (double)pc;
+        one = pc == 1.0f;
+    } else {
+        double pc = d64 > 0 ? 1.0 / sqrt(d64) : 0.0;
+        A.diag[c] = d64;
+        A.pc64[c] = pc;
+        A.pc32[c] = (float)pc;
+        one = pc == 1.0;
+    }
+    if (one) atomicAdd(&A.sc[s].ones, 1);
+}
+
+__global__ void k_fl_write(PcgArgs A, const uint32_t* pred, const uint32_t* scan) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= A.S.nc) return;
+    if (pred[c]) const_cast<uint32_t*>(A.fl)[scan[c]] = (uint32_t)c;
+}
+
+__global__ void k_pcg_tables(PcgArgs A, const uint32_t* scan) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int k = A.S.k;
+    long long* flp = const_cast<long long*>(A.fl_pref);
+    long long* chp = const_cast<long long*>(A.ch_pref);
+    long long acc = 0;
+    int any_ordered = 0;
+    for (int s = 0; s <= k; ++s) flp[s] = scan[A.S.c_pref[s]];
+    for (int s = 0; s < k; ++s) {
+        chp[s] = acc;
+        long long nf = flp[s + 1] - flp[s];
+        acc += (nf + A.chunk - 1) / A.chunk;
+        PcgScene& P = A.sc[s];
+        P.nf = (int)nf;
+        P.ordered = nf > 0 && (A.precond == ARIEL_PRECOND_MIC0 || P.ones > 0);
+        any_ordered |= P.ordered;
+    }
+    chp[k] = acc;
+    A.ctl->all_done = 0;
+    A.ctl->all_inner_done = 0;
+    A.ctl->any_ordered = any_ordered;
+}
+
+// ------------------------------------------------------------------------------------------
+// Ordered preconditioner: one block sweeps a scene's i+j+k hyperplanes (forward) or in
+// reverse (backward); cells of one plane are independent.
+// ------------------------------------------------------------------------------------------
+template <class F>
+__device__ void hyperplanes(int n, bool reverse, F&& f) {
+    const int nd = 3 * (n - 1) + 1;
+    for (int di = 0; di < nd; ++di) {
+        const int d = reverse ? nd - 1 - di : di;
+        const int ilo = max(0, d - 2 * (n - 1)), ihi = min(n - 1, d);
+        const long long cnt = (long long)(ihi - ilo + 1) * n;
+        for (long long idx = threadIdx.x; idx < cnt; idx += blockDim.x) {
+            int i = ilo + (int)(idx / n), j = (int)(idx % n);
+            int k = d - i - j;
+            if (k >= 0 && k < n) f(i, j, k);
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T ldv(const T* p) {
+    return __ldcg(p);
+}
+
+__device__ void ordered_build(const PcgArgs& A, int s) {
+    const DevState& S = A.S;
+    const SceneDev& D = S.scenes[s];
+    const int n = D.n;
+    const long long cb = D.c_begin;
+    auto cid = [&](int i, int j, int k) { return cb + ((long long)i * n + j) * n + k; };
+    auto fluid = [&](int i, int j, int k) {
+        return i >= 0 && j >= 0 && k >= 0 && i < n && j < n && k < n && S.flags[cid(i, j, k)] == ARIEL_FLUID;
+    };
+    if (A.precond == ARIEL_PRECOND_MIC0) {
+        const double tau = A.tau, sigma = A.sigma;
+        hyperplanes(n, false, [&](int i, int j, int k) {
+            long long c = cid(i, j, k);
+            if (S.flags[c] != ARIEL_FLUID) return;
+            double e = A.diag[c];
+            if (fluid(i - 1, j, k)) {
+                double p = ldv(A.pc64 + cid(i - 1, j, k));
+                double ap = -1.0;
+                double oth = (fluid(i - 1, j + 1, k) ? -1.0 : 0.0) + (fluid(i - 1, j, k + 1) ? -1.0 : 0.0);
+                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
+            }
+            if (fluid(i, j - 1, k)) {
+                double p = ldv(A.pc64 + cid(i, j - 1, k));
+                double ap = -1.0;
+                double oth = (fluid(i + 1, j - 1, k) ? -1.0 : 0.0) + (fluid(i, j - 1, k + 1) ? -1.0 : 0.0);
+                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
+            }
+            if (fluid(i, j, k - 1)) {
+                double p = ldv(A.pc64 + cid(i, j, k - 1));
+                double ap = -1.0;
+                double oth = (fluid(i + 1, j, k - 1) ? -1.0 : 0.0) + (fluid(i, j + 1, k - 1) ? -1.0 : 0.0);
+                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
+            }
+            if (e < sigma * A.diag[c]) e = A.diag[c];
+            double pc = e > 0 ? 1.0 / sqrt(e) : 0.0;
+            A.pc64[c] = pc;
+            A.pc32[c] = (float)pc;
+        });
+        return;
+    }
+    if (A.mode == kRef32) {
+        // BuildPreconditioner in serial order, fp32 (solver.inl:104-135)
+        hyperplanes(n, false, [&](int i, int j, int k) {
+            long long c = cid(i, j, k);
+            if (S.flags[c] != ARIEL_FLUID) return;
+            auto term = [&](int a, int b, int cc) {
+                float ar = fluid(a, b, cc) ? -1.0f : 0.0f;  // ARef
+                float pr = 0.0f;                           // PRef: value only if == 1.0f
+                if (a >= 0 && b >= 0 && cc >= 0 && a < n && b < n && cc < n) {
+                    float v = ldv(A.pc32 + cid(a, b, cc));
+                    if (v == 1.0f) pr = v;
+                }
+                return ar * pr;
+            };
+            float left = term(i - 1, j, k), bottom = term(i, j - 1, k), back = term(i, j, k - 1);
+            float diag = (float)A.diag[c];
+            float e = diag - (left * left) - (bottom * bottom) - (back * back);
+            float pc = 0.0f;
+            if (diag > 0) {
+                if (e < 0.25f * diag) e = diag;
+                pc = 1.0f / sqrtf(e);
+            }
+            A.pc32[c] = pc;
+            A.pc64[c] = (double)pc;
+        });
+        return;
+    }
+    hyperplanes(n, false, [&](int i, int j, int k) {
+        long long c = cid(i, j, k);
+        if (S.flags[c] != ARIEL_FLUID) return;
+        auto term = [&](int a, int b, int cc) {
+            return (fluid(a, b, cc) && ldv(A.pc64 + cid(a, b, cc)) == 1.0) ? -1.0 : 0.0;
+        };
+        double left = term(i - 1, j, k), bottom = term(i, j - 1, k), back = term(i, j, k - 1);
+        double dg = A.diag[c];
+        double e = dg - left * left - bottom * bottom - back * back;
+        double pc = 0.0;
+        if (dg > 0) {
+            if (e < 0.25 * dg) e = dg;
+            pc = 1.0 / sqrt(e);
+        }
+        A.pc64[c] = pc;
+        A.pc32[c] = (float)pc;
+    });
+}
+
+// z = M^-1 r by ordered forward and backward sweeps over one scene (T = vector type).
+template <class T>
+__device__ void ordered_apply(const PcgArgs& A, int s, const T* r, T* z, T* q, const T* pc, bool ref32) {
+    const DevState& S = A.S;
+    const SceneDev& D = S.scenes[s];
+    const int n = D.n;
+    const long long cb = D.c_begin;
+    const bool mic = A.precond == ARIEL_PRECOND_MIC0;
+    auto cid = [&](int i, int j, int k) { return cb + ((long long)i * n + j) * n + k; };
+    auto fluid = [&](int i, int j, int k) {
+        return i >= 0 && j >= 0 && k >= 0 && i < n && j < n && k < n && S.flags[cid(i, j, k)] == ARIEL_FLUID;
+    };
+    hyperplanes(n, false, [&](int i, int j, int k) {
+        long long c = cid(i, j, k);
+        if (S.flags[c] != ARIEL_FLUID) return;
+        const int lo[3][3] = {{i - 1, j, k}, {i, j - 1, k}, {i, j, k - 1}};
+        T t = ldv(r + c);
+        for (int m = 0; m < 3; ++m) {
+            if (!fluid(lo[m][0], lo[m][1], lo[m][2])) continue;
+            long long qc = cid(lo[m][0], lo[m][1], lo[m][2]);
+            T pq = ldv(pc + qc), qq = ldv(q + qc);
+            if (mic)
+                t -= (T)-1.0 * pq * qq;
+            else if (pq == (T)1.0 && qq == (T)1.0)
+                t -= (T)-1.0;  // ARef*PRef(P)*PRef(Q) = -1
+        }
+        q[c] = t * ldv(pc + c);
+    });
+    hyperplanes(n, true, [&](int i, int j, int k) {
+        long long c = cid(i, j, k);
+        if (S.flags[c] != ARIEL_FLUID) return;
+        const int hi[3][3] = {{i + 1, j, k}, {i, j + 1, k}, {i, j, k + 1}};
+        T pcc = ldv(pc + c);
+        T t = ldv(q + c);
+        for (int m = 0; m < 3; ++m) {
+            if (!fluid(hi[m][0], hi[m][1], hi[m][2])) continue;
+            long long qc = cid(hi[m][0], hi[m][1], hi[m][2]);
+            T zq = ldv(z + qc);
+            if (mic)
+                t -= (T)-1.0 * pcc * zq;
+            else if (pcc == (T)1.0 && zq == (T)1.0)
+                t -= (T)-1.0;
+        }
+        z[c] = t * pcc;
+    });
+    (void)ref32;
+}
+
+// ------------------------------------------------------------------------------------------
+// Operators.
+// ------------------------------------------------------------------------------------------
+// ComputeAx for one FLUID cell with the reference's exact expression (solver.inl:196-230).
+// `sv(q)` yields the vector value at FLUID cell q; xc is the value at c.
+template <class SV>
+__device__ __forceinline__ float ax_ref32(const DevState& S, const SceneDev& D, long long c, float xc, SV&& sv) {
+    const int n = D.n;
+    int i, j, k;
+    cell_ijk(c - D.c_begin, n, i, j, k);
+    const float Lc = S.L[c];
+    auto xref = [&](int pi, int pj, int pk) -> float {
+        int a = min(max(0, pi), n - 1), b = min(max(0, pj), n - 1), cc = min(max(0, pk), n - 1);
+        long long q = D.c_begin + ((long long)a * n + b) * n + cc;
+        uint8_t t = S.flags[q];
+        if (t == ARIEL_FLUID) return q == c ? xc : sv(q);
+        if (t == ARIEL_SOLID) return xc;
+        if (D.subcell) return S.L[q] / gmin(1.0e-6f, Lc) * xc;
+        return 0.0f;
+    };
+    float result = (6.0f * xc - xref(i + 1, j, k) - xref(i - 1, j, k) - xref(i, j + 1, k) - xref(i, j - 1, k) -
+                    xref(i, j, k + 1) - xref(i, j, k - 1)) /
+                   D.ax_h;
+    return result;
+}
+
+__device__ __forceinline__ long long nb_off(int d, int n) {
+    const long long nn = (long long)n * n;
+    switch (d) {
+        case 0: return -nn;
+        case 1: return nn;
+        case 2: return -(long long)n;
+        case 3: return (long long)n;
+        case 4: return -1;
+        default: return 1;
+    }
+}
+
+// Diagonal form (FP64 and the MIXED fp32 inner operator): (diag*x_c - sum_FLUID x_q) / h.
+template <class T, class SV>
+__device__ __forceinline__ T ax_diag(const PcgArgs& A, const SceneDev& D, long long c, T xc, SV&& sv) {
+    const uint8_t m = A.mask[c];
+    T acc = (T)A.diag[c] * xc;
+#pragma unroll
+    for (int d = 0; d < 6; ++d)
+        if (m & (1u << d)) acc -= sv(c + nb_off(d, D.n));
+    const T scale = (T)(1.0 / (double)D.ax_h);
+    return acc * scale;
+}
+
+// ------------------------------------------------------------------------------------------
+// The persistent solve.
+// ------------------------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
+    using T = typename VT<MODE>::T;
+    const DevState& S = A.S;
+    const int k = S.k;
+    __shared__ long long fl_s[kMaxScenes + 1], ch_s[kMaxScenes + 1];
+    for (int i = threadIdx.x; i <= k; i += blockDim.x) {
+        fl_s[i] = A.fl_pref[i];
+        ch_s[i] = A.ch_pref[i];
+    }
+    __syncthreads();
+    const long long nch = ch_s[k];
+    const long long MC = A.max_chunks;
+    double* part0 = A.partial;
+    double* part1 = A.partial + MC;
+    PcgScene* SC = A.sc;
+    T* r = (T*)A.r;
+    T* z = (T*)A.z;
+    T* q = (T*)A.q;
+    T* sb[2] = {(T*)A.s0, (T*)A.s1};
+    T* ordq = (T*)A.ordq;
+    const T* pcv = MODE == kFp64 ? (const T*)(const void*)A.pc64 : (const T*)(const void*)A.pc32;
+    // x of the working solve: P (REF32), P64 (FP64), d32 (MIXED inner correction)
+    T* x = MODE == kRef32 ? (T*)(void*)S.P : (MODE == kFp64 ? (T*)(void*)S.P64 : (T*)(void*)A.d32);
+    const bool any_ordered = __ldcg(&A.ctl->any_ordered) != 0;
+    const unsigned long long tmo = A.timeout_ns;
+    __shared__ int s_active;
+
+    auto chunk_range = [&](long long ch, int& s, long long& t0, long long& t1) {
+        s = find_scene(ch_s, k, ch);
+        t0 = fl_s[s] + (ch - ch_s[s]) * A.chunk;
+        t1 = min(t0 + (long long)A.chunk, fl_s[s + 1]);
+    };
+    auto write_part = [&](long long ch, double a, double b) {
+        block_sum2(a, b);
+        if (threadIdx.x == 0) {
+            part0[ch] = a;
+            part1[ch] = b;
+        }
+    };
+    // elementwise preconditioner of the reference ((r*pc)*pc) for non-ordered scenes
+    auto precond_elem = [&](long long c, T rv) -> T { return (rv * ldv(pcv + c)) * ldv(pcv + c); };
+
+    // ---- Phase 0: ordered preconditioner build -------------------------------------------
+    if (any_ordered) {
+        for (int s = blockIdx.x; s < k; s += gridDim.x)
+            if (__ldcg(&SC[s].ordered)) ordered_build(A, s);
+        if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
+    }
+
+    int outer = 0;
+    while (true) {
+        // ---- Phase R: residual r = b - A x and |b|^2 ----------------------------------------
+        for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+            int s;
+            long long t0, t1;
+            chunk_range(ch, s, t0, t1);
+            const SceneDev& D = S.scenes[s];
+            double a0 = 0.0, a1 = 0.0;
+            if (!__ldcg(&SC[s].done)) {
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = A.fl[t];
+                    double bv = (double)S.D[c];
+                    if (MODE == kRef32) {
+                        float xc = ldv(S.P + c);
+                        float ax = ax_ref32(S, D, c, xc, [&](long long qq) { return ldv(S.P + qq); });
+                        float rv = S.D[c] + (-1.0f) * ax;  // Op(A, D, Z, R, -1)
+                        r[c] = (T)rv;
+                        a0 += (double)rv * (double)rv;
+                    } else {
+                        double xc = ldv(S.P64 + c);
+                        double ax = ax_diag<double>(A, D, c, xc, [&](long long qq) { return ldv(S.P64 + qq); });
+                        double rv = bv - ax;
+                        if (MODE == kMixed)
+                            A.r64[c] = rv;
+                        else
+                            r[c] = (T)rv;
+                        a0 += rv * rv;
+                    }
+                    a1 += bv * bv;
+                }
+            }
+            write_part(ch, a0, a1);
+        }
+        bool ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+            if (threadIdx.x == 0) s_active = 0;
+            __syncthreads();
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            for (int s = wid; s < k; s += blockDim.x / 32) {
+                double rr = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                double bb = scene_sum(part1, ch_s[s], ch_s[s + 1]);
+                if (lane == 0) {
+                    PcgScene P = load_sc(SC + s);
+                    if (!P.done) {
+                        const int n = S.scenes[s].n;
+                        if (outer == 0) P.bb = bb;
+                        P.rr_out = rr;
+                        if (MODE == kMixed) P.outer += 1;
+                        double lim2 = A.tol * A.tol * P.bb;
+                        double abs_eps = (double)(1.0e-2f * (float)(n * n * n));
+                        bool conv = false;
+                        if (A.stop_rule == ARIEL_STOP_REL)
+                            conv = rr <= lim2;
+                        else if (MODE == kMixed)
+                            conv = outer > 0 && rr <= abs_eps;
+                        if (P.nf == 0) conv = true;
+                        int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+                        if (conv) {
+                            P.done = 1;
+                            P.converged = 1;
+                        } else if (MODE == kMixed && (P.outer > A.max_outer || P.iters >= cap)) {
+                            P.done = 1;
+                            P.converged = 0;
+                        }
+                        if (!P.done) {
+                            P.inner_done = 0;
+                            P.rr = rr;
+                            if (MODE == kMixed) {
+                                double t1 = A.inner_tol * A.inner_tol * rr;
+                                double t2 = A.stop_rule == ARIEL_STOP_REL ? 0.25 * lim2 : 0.0;
+                                P.target = t1 > t2 ? t1 : t2;
+                            } else {
+                                P.target = A.stop_rule == ARIEL_STOP_REL ? lim2 : abs_eps;
+                            }
+                            atomicAdd(&s_active, 1);
+                        } else {
+                            P.inner_done = 1;
+                        }
+                        SC[s] = P;
+                    }
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                A.ctl->all_done = s_active == 0;
+                A.ctl->all_inner_done = s_active == 0;
+            }
+        });
+        if (!ok) return;
+        if (__ldcg(&A.ctl->all_done)) break;
+
+        // ---- Phase I: z = M r, s = z, rho = z.r (MIXED: r32 = r64, d = 0) ------------------
+        for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+            int s;
+            long long t0, t1;
+            chunk_range(ch, s, t0, t1);
+            const bool active = !__ldcg(&SC[s].inner_done);
+            const bool ord = __ldcg(&SC[s].ordered) != 0;
+            double a0 = 0.0;
+            if (active) {
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = A.fl[t];
+                    T rv;
+                    if (MODE == kMixed) {
+                        rv = (T)A.r64[c];
+                        r[c] = rv;
+                        x[c] = (T)0;
+                    } else {
+                        rv = ldv(r + c);
+                    }
+                    if (!ord) {
+                        T zv = precond_elem(c, rv);
+                        z[c] = zv;
+                        sb[0][c] = zv;
+                        a0 += (double)zv * (double)rv;
+                    }
+                }
+            }
+            if (!ord) write_part(ch, a0, 0.0);
+        }
+        if (any_ordered) {
+            if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
+            for (int s = blockIdx.x; s < k; s += gridDim.x) {
+                if (!__ldcg(&SC[s].ordered) || __ldcg(&SC[s].inner_done)) continue;
+                ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
+                double a0 = 0.0;
+                for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
+                    long long c = A.fl[t];
+                    T zv = ldv(z + c);
+                    sb[0][c] = zv;
+                    a0 += (double)zv * (double)ldv(r + c);
+                }
+                double b0 = 0.0;
+                block_sum2(a0, b0);
+                if (threadIdx.x == 0)
+                    for (long long ch = ch_s[s]; ch < ch_s[s + 1]; ++ch) {
+                        part0[ch] = ch == ch_s[s] ? a0 : 0.0;
+                        part1[ch] = 0.0;
+                    }
+            }
+        }
+        ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+            const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            for (int s = wid; s < k; s += blockDim.x / 32) {
+                double rho = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                if (lane == 0) {
+                    PcgScene P = load_sc(SC + s);
+                    if (!P.inner_done) {
+                        P.rho = rho;
+                        P.rho32 = (float)rho;
+                        SC[s] = P;
+                    }
+                }
+            }
+        });
+        if (!ok) return;
+
+        // ---- CG iterations -------------------------------------------------------------------
+        for (int it = 0;; ++it) {
+            T* s_cur = sb[it & 1];
+            T* s_prev = sb[(it + 1) & 1];
+            // Phase A: s = z + beta s (it > 0), q = A s, s.q
+            for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                int s;
+                long long t0, t1;
+                chunk_range(ch, s, t0, t1);
+                const SceneDev& D = S.scenes[s];
+                double a0 = 0.0;
+                if (!__ldcg(&SC[s].inner_done)) {
+                    const double beta = __ldcg(&SC[s].beta);
+                    const float beta32 = __ldcg(&SC[s].beta32);
+                    const T bt = MODE == kRef32 ? (T)beta32 : (T)beta;
+                    auto sval = [&](long long qq) -> T {
+                        if (it == 0) return ldv(s_cur + qq);
+                        return ldv(z + qq) + bt * ldv(s_prev + qq);  // Op(A, Z, S, S, beta)
+                    };
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = A.fl[t];
+                        T sc_ = sval(c);
+                        if (it > 0) s_cur[c] = sc_;
+                        T qv;
+                        if (MODE == kRef32)
+                            qv = ax_ref32(S, D, c, sc_, sval);
+                        else
+                            qv = ax_diag<T>(A, D, c, sc_, sval);
+                        q[c] = qv;
+                        a0 += (double)sc_ * (double)qv;
+                    }
+                }
+                write_part(ch, a0, 0.0);
+            }
+            ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+                const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+                for (int s = wid; s < k; s += blockDim.x / 32) {
+                    double sq = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                    if (lane == 0) {
+                        PcgScene P = load_sc(SC + s);
+                        if (!P.inner_done) {
+                            P.alpha = sq != 0.0 ? P.rho / sq : 0.0;
+                            float sq32 = (float)sq;
+                            P.alpha32 = sq32 != 0.0f ? P.rho32 / sq32 : 0.0f;
+                            SC[s] = P;
+                        }
+                    }
+                }
+            });
+            if (!ok) return;
+            // Phase B: x += alpha s, r -= alpha q, r.r; z = M r, z.r (fused when no scene is
+            // ordered)
+            for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                int s;
+                long long t0, t1;
+                chunk_range(ch, s, t0, t1);
+                double a0 = 0.0, a1 = 0.0;
+                if (!__ldcg(&SC[s].inner_done)) {
+                    const T al = MODE == kRef32 ? (T)__ldcg(&SC[s].alpha32) : (T)__ldcg(&SC[s].alpha);
+                    const bool fuse = !any_ordered;
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = A.fl[t];
+                        T sv = ldv(s_cur + c);
+                        T xv = ldv(x + c) + al * sv;
+                        T rv = ldv(r + c) + (-al) * ldv(q + c);
+                        x[c] = xv;
+                        r[c] = rv;
+                        a0 += (double)rv * (double)rv;
+                        if (fuse) {
+                            T zv = precond_elem(c, rv);
+                            z[c] = zv;
+                            a1 += (double)zv * (double)rv;
+                        }
+                    }
+                }
+                write_part(ch, a0, a1);
+            }
+            if (any_ordered) {
+                ok = grid_barrier(A.bar, S.dev_error, tmo, NoLeader{});
+                if (!ok) return;
+                for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                    int s;
+                    long long t0, t1;
+                    chunk_range(ch, s, t0, t1);
+                    if (__ldcg(&SC[s].ordered)) continue;
+                    double a1 = 0.0;
+                    if (!__ldcg(&SC[s].inner_done)) {
+                        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                            long long c = A.fl[t];
+                            T rv = ldv(r + c);
+                            T zv = precond_elem(c, rv);
+                            z[c] = zv;
+                            a1 += (double)zv * (double)rv;
+                        }
+                    }
+                    double b0 = 0.0;
+                    block_sum2(a1, b0);
+                    if (threadIdx.x == 0) part1[ch] = a1;
+                }
+                for (int s = blockIdx.x; s < k; s += gridDim.x) {
+                    if (!__ldcg(&SC[s].ordered) || __ldcg(&SC[s].inner_done)) continue;
+                    ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
+                    double a1 = 0.0;
+                    for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
+                        long long c = A.fl[t];
+                        a1 += (double)ldv(z + c) * (double)ldv(r + c);
+                    }
+                    double b0 = 0.0;
+                    block_sum2(a1, b0);
+                    if (threadIdx.x == 0)
+                        for (long long ch = ch_s[s]; ch < ch_s[s + 1]; ++ch) part1[ch] = ch == ch_s[s] ? a1 : 0.0;
+                }
+            }
+            ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+                if (threadIdx.x == 0) s_active = 0;
+                __syncthreads();
+                const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+                for (int s = wid; s < k; s += blockDim.x / 32) {
+                    double rr = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                    double rho2 = scene_sum(part1, ch_s[s], ch_s[s + 1]);
+                    if (lane == 0) {
+                        PcgScene P = load_sc(SC + s);
+                        if (!P.inner_done) {
+                            const int n = S.scenes[s].n;
+                            P.iters += 1;
+                            P.rr = rr;
+                            const int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+                            bool conv = MODE == kRef32 ? ((float)rr <= (float)P.target) : (rr <= P.target);
+                            if (conv || P.iters >= cap) {
+                                P.inner_done = 1;
+                                if (MODE != kMixed) {
+                                    P.done = 1;
+                                    P.converged = conv;
+                                }
+                            } else {
+                                P.beta = P.rho != 0.0 ? rho2 / P.rho : 0.0;
+                                P.rho = rho2;
+                                float r32 = (float)rho2;
+                                P.beta32 = P.rho32 != 0.0f ? r32 / P.rho32 : 0.0f;
+                                P.rho32 = r32;
+                                atomicAdd(&s_active, 1);
+                            }
+                            SC[s] = P;
+                        }
+                    }
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) A.ctl->all_inner_done = s_active == 0;
+            });
+            if (!ok) return;
+            if (__ldcg(&A.ctl->all_inner_done)) break;
+        }
+
+        if (MODE != kMixed) break;
+        // ---- MIXED: x64 += d ------------------------------------------------------------------
+        for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+            int s;
+            long long t0, t1;
+            chunk_range(ch, s, t0, t1);
+            if (__ldcg(&SC[s].done)) continue;
+            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                long long c = A.fl[t];
+                S.P64[c] = ldv(S.P64 + c) + (double)ldv(x + c);
+            }
+        }
+        if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
+        ++outer;
+    }
+
+    // ---- totals (block 0; every scene is done here) ---------------------------------------
+    if (blockIdx.x == 0) {
+        for (int s = threadIdx.x; s < k; s += blockDim.x) {
+            PcgScene P = load_sc(SC + s);
+            PcgTotals& T = A.totals[s];
+            T.solves += 1;
+            T.iterations += P.iters;
+            T.outer += MODE == kMixed ? P.outer : 1;
+            T.cell_iterations += (double)P.nf * (double)P.iters;
+            T.cell_outer += (double)P.nf * (double)(MODE == kMixed ? P.outer : 1);
+            T.not_converged += P.converged ? 0 : 1;
+        }
+    }
+    // ---- output: fp32 pressure from the fp64 solution ---------------------------------------
+    if (MODE != kRef32) {
+        for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+            int s;
+            long long t0, t1;
+            chunk_range(ch, s, t0, t1);
+            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                long long c = A.fl[t];
+                S.P[c] = (float)ldv(S.P64 + c);
+            }
+        }
+    }
+}
+
+__global__ void k_barrier_selftest(Barrier* bar, int* err, unsigned long long tmo) {
+    // Nobody releases this barrier, so every block must give up when its budget runs out.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned g = ld_acquire_u32(&bar->gen);
+        atomicAdd(&bar->count, 1u);
+        unsigned long long t0 = gtimer();
+        while (ld_acquire_u32(&bar->gen) == g) {
+            if (gtimer() - t0 > tmo) {
+                atomicExch(&bar->error, 1);
+                atomicExch(err, 1);
+                break;
+            }
+            __nanosleep(1000);
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan, void* scan_tmp, cudaStream_t st) {
+    const DevState& S = A.S;
+    cudaMemsetAsync(A.sc, 0, sizeof(PcgScene) * (size_t)S.k, st);
+    cudaMemsetAsync(A.ctl, 0, sizeof(PcgCtl), st);
+    cudaMemsetAsync(A.bar, 0, sizeof(Barrier), st);
+    if (S.nc > 0) {
+        k_prep_cells<<<grid_for(S.nc), kBlock, 0, st>>>(A, pred);
+        count_launch();
+    }
+    cudaError_t e = launch_scan_u32(pred, scan, S.nc, scan_tmp, st);
+    if (e != cudaSuccess) return e;
+    if (S.nc > 0) {
+        k_fl_write<<<grid_for(S.nc), kBlock, 0, st>>>(A, pred, scan);
+        count_launch();
+    }
+    k_pcg_tables<<<1, 32, 0, st>>>(A, scan);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t coop_launch(const PcgArgs& A, int nblocks, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nblocks);
+    cfg.blockDim = dim3(kPcgThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg<MODE>, A);
+    count_launch();
+    return e;
+}
+
+cudaError_t launch_pcg_solve(const PcgArgs& A, int nblocks, cudaStream_t st) {
+    switch (A.mode) {
+        case kRef32: return coop_launch<kRef32>(A, nblocks, st);
+        case kFp64: return coop_launch<kFp64>(A, nblocks, st);
+        default: return coop_launch<kMixed>(A, nblocks, st);
+    }
+}
+
+int pcg_max_blocks(int device, int mode) {
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e;
+    if (mode == kRef32)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kRef32>, kPcgThreads, 0);
+    else if (mode == kFp64)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kFp64>, kPcgThreads, 0);
+    else
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kMixed>, kPcgThreads, 0);
+    if (e != cudaSuccess || per < 1) per = 1;
+    // Two blocks per SM cover the FLUID chunks of the bench sizes; more blocks only lengthen
+    // every grid barrier.
+    return sms * (per < 2 ? per : 2);
+}
+
+cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long timeout_ns, cudaStream_t st) {
+    cudaMemsetAsync(bar, 0, sizeof(Barrier), st);
+    k_barrier_selftest<<<2, 32, 0, st>>>(bar, err, timeout_ns);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace ariel

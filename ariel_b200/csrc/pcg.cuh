@@ -1,0 +1,101 @@
+// pcg.cuh -- pressure-solve data shared by pcg.cu and host.cu.
+#pragma once
+
+#include "state.cuh"
+
+namespace ariel {
+
+enum PcgMode { kRef32 = 0, kFp64 = 1, kMixed = 2 };
+
+// Per-scene solver scalars, written by the leader block of each grid barrier.
+struct PcgScene {
+    double bb;        // |b|^2 over FLUID cells
+    double rr;        // r.r of the working (inner) residual
+    double rho;       // z.r
+    double alpha, beta;
+    double rr_out;    // |b - A x|^2 at the last outer residual (FP64/MIXED true residual)
+    double target;    // stop threshold on rr of the current (inner) solve
+    float alpha32, beta32, rho32, pad32;
+    int iters;        // CG iterations (summed over inner solves)
+    int outer;        // refinement sweeps
+    int done;         // whole solve finished
+    int inner_done;   // current inner solve finished
+    int converged;
+    int ordered;      // preconditioner needs the ordered (wavefront) path
+    int ones;         // FLUID cells whose order-free REF preconditioner value is exactly 1
+    int nf;           // FLUID cells
+    int pad[2];
+};
+static_assert(sizeof(PcgScene) % 16 == 0, "PcgScene is copied as 16-byte words");
+
+// Accumulated over solves (reset by the host); written by the leader when a scene finishes.
+struct PcgTotals {
+    long long solves, iterations, outer;
+    double cell_iterations, cell_outer;
+    long long not_converged, pad;
+};
+
+struct PcgCtl {
+    int all_done;
+    int all_inner_done;
+    int any_ordered;
+    int pad;
+};
+
+struct Barrier {
+    unsigned count;
+    unsigned gen;
+    int error;
+    int pad;
+};
+
+struct PcgArgs {
+    DevState S;
+    int mode;
+    int precond;
+    int stop_rule;
+    int max_iters;     // <=0: n^3 per scene
+    int max_outer;
+    int chunk;         // FLUID cells per chunk
+    double tol;
+    double inner_tol;
+    double tau, sigma;
+    unsigned long long timeout_ns;
+    // FLUID list
+    const uint32_t* fl;        // packed FLUID cells, scene by scene, ascending
+    const long long* fl_pref;  // k+1
+    const long long* ch_pref;  // k+1 chunk begins
+    // per-cell operator data (dense over packed cells)
+    uint8_t* mask;   // bit d set: neighbour d (-x,+x,-y,+y,-z,+z) is FLUID
+    double* diag;    // ADiag (fp32 value for REF32, fp64 otherwise)
+    double* pc64;    // preconditioner values
+    float* pc32;
+    // vectors (dense over packed cells); element type per mode
+    void* r;
+    void* z;
+    void* s0;
+    void* s1;
+    void* q;
+    void* ordq;      // forward-sweep scratch of the ordered preconditioner
+    double* r64;     // MIXED outer residual
+    float* d32;      // MIXED inner correction
+    double* partial; // 3 * max chunks
+    long long max_chunks;
+    PcgScene* sc;
+    PcgTotals* totals;
+    PcgCtl* ctl;
+    Barrier* bar;
+};
+
+// Build the FLUID list, per-cell operator data and chunk table; zero non-FLUID pressure.
+cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan, void* scan_tmp, cudaStream_t st);
+// The cooperative persistent PCG kernel.
+cudaError_t launch_pcg_solve(const PcgArgs& A, int nblocks, cudaStream_t st);
+// Blocks of the persistent kernel that fit on the device at once.
+int pcg_max_blocks(int device, int mode);
+// Bounded-wait self test (one arrival missing).
+cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long timeout_ns, cudaStream_t st);
+
+constexpr int kPcgThreads = 256;
+
+}  // namespace ariel

@@ -1,0 +1,221 @@
+"""Python mirror of the reference's `fluidCore::FlipSim` (src/sim/flip.hpp:20-66) over the C ABI.
+
+    sim = FlipSim(maxres=64, density=0.5, stepsize=1/240, scene=dambreak(64), verbose=False)
+    sim.Init(); sim.Step(False, False, False); particles = sim.GetParticles()
+
+Construction, Init and Step follow the reference's names and meaning; the state lives on the
+B200 and GetParticles copies it to host numpy arrays.  `Batch` steps several scenes together.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+from ._lib import ArielError, check, lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def grid_shape(n, which):
+    if which in (A.GRID_UX, A.GRID_PREV_UX):
+        return (n + 1, n, n), np.float32
+    if which in (A.GRID_UY, A.GRID_PREV_UY):
+        return (n, n + 1, n), np.float32
+    if which in (A.GRID_UZ, A.GRID_PREV_UZ):
+        return (n, n, n + 1), np.float32
+    if which == A.GRID_A:
+        return (n, n, n), np.int32
+    if which == A.GRID_P64:
+        return (n, n, n), np.float64
+    return (n, n, n), np.float32
+
+
+class Batch:
+    """k scenes stepped together (one launch per stage over a packed index space)."""
+
+    def __init__(self, descs, params=None):
+        self.L = lib()
+        if params is None:
+            params = A.params_default()
+        self.params = params
+        arr = (A.AsimSceneDesc * len(descs))(*descs)
+        h = C.c_void_p()
+        if len(descs) == 1:
+            check(self.L.ariel_create(C.byref(arr[0]), C.byref(params), C.byref(h)), "ariel_create")
+        else:
+            check(self.L.ariel_create_batch(arr, len(descs), C.byref(params), C.byref(h)), "ariel_create_batch")
+        self.h = h
+        self.descs = list(descs)
+        self.k = len(descs)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ariel_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- lifecycle ---------------------------------------------------------------------
+    def init(self):
+        check(self.L.ariel_init(self.h), "ariel_init")
+
+    def step(self, n=1):
+        check(self.L.ariel_step(self.h, n), "ariel_step")
+
+    def stage(self, s):
+        check(self.L.ariel_stage(self.h, s), "ariel_stage")
+
+    def synchronize(self):
+        check(self.L.ariel_synchronize(self.h), "ariel_synchronize")
+
+    # -- accessors ---------------------------------------------------------------------
+    def dim(self, scene=0):
+        return self.descs[scene].dim
+
+    def count(self, scene=0):
+        n = C.c_int64()
+        check(self.L.ariel_particle_count(self.h, scene, C.byref(n)), "ariel_particle_count")
+        return n.value
+
+    def get_particles(self, scene=0):
+        n = self.count(scene)
+        pos = np.zeros((n, 3), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        den = np.zeros(n, np.float32)
+        mass = np.zeros(n, np.float32)
+        typ = np.zeros(n, np.int32)
+        check(self.L.ariel_get_particles(self.h, scene, _p(pos), _p(vel), _p(den), _p(mass), _p(typ)),
+              "ariel_get_particles")
+        return dict(pos=pos, vel=vel, density=den, mass=mass, type=typ)
+
+    def get_positions_velocities(self, pos, vel, scene=0):
+        check(self.L.ariel_get_particles(self.h, scene, _p(pos), _p(vel), None, None, None), "ariel_get_particles")
+
+    def set_particles(self, pos, vel, mass, typ, scene=0):
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        mass = np.ascontiguousarray(mass, np.float32)
+        typ = np.ascontiguousarray(typ, np.int32)
+        check(self.L.ariel_set_particles(self.h, scene, len(mass), _p(pos), _p(vel), _p(mass), _p(typ)),
+              "ariel_set_particles")
+
+    def get_cells(self, scene=0):
+        n = self.count(scene)
+        d = self.dim(scene)
+        pc = np.zeros(n, np.int32)
+        cc = np.zeros(d ** 3, np.int32)
+        check(self.L.ariel_get_cells(self.h, scene, _p(pc), _p(cc)), "ariel_get_cells")
+        return pc, cc
+
+    def get_grid(self, which, scene=0):
+        shape, dt = grid_shape(self.dim(scene), which)
+        a = np.zeros(shape, dt)
+        check(self.L.ariel_get_grid(self.h, scene, which, _p(a), a.nbytes), "ariel_get_grid")
+        return a
+
+    def set_grid(self, which, a, scene=0):
+        shape, dt = grid_shape(self.dim(scene), which)
+        a = np.ascontiguousarray(a, dt).reshape(shape)
+        check(self.L.ariel_set_grid(self.h, scene, which, _p(a), a.nbytes), "ariel_set_grid")
+
+    def stats(self, scene=0):
+        st = A.AsimStats()
+        check(self.L.ariel_stats(self.h, scene, C.byref(st)), "ariel_stats")
+        return st
+
+    def max_density(self, scene=0):
+        v = C.c_float()
+        check(self.L.ariel_get_max_density(self.h, scene, C.byref(v)), "ariel_get_max_density")
+        return v.value
+
+    def upload_state(self, pos, vel, scene=0):
+        """Asynchronous H2D of xyz positions/velocities (keep the buffers alive until the
+        next synchronising call)."""
+        check(self.L.ariel_upload_state(self.h, scene, _p(pos), _p(vel)), "ariel_upload_state")
+
+    def download_state(self, pos, vel, scene=0):
+        check(self.L.ariel_download_state(self.h, scene, _p(pos), _p(vel)), "ariel_download_state")
+
+    def timing_reset(self):
+        check(self.L.ariel_timing_reset(self.h), "ariel_timing_reset")
+
+    def timing(self, max_steps=4096):
+        ms = np.zeros(A.STAGE_COUNT, np.float64)
+        solve_k = C.c_double()
+        steps = np.zeros(max_steps, np.float64)
+        n = C.c_int32()
+        check(self.L.ariel_timing_get(self.h, _p(ms), C.byref(solve_k), _p(steps), max_steps, C.byref(n)),
+              "ariel_timing_get")
+        return dict(stage_ms=ms, solve_kernel_ms=solve_k.value, steps=n.value,
+                    step_ms=steps[:min(n.value, max_steps)].copy())
+
+    def solver_totals(self, scene=0):
+        t = A.AsimSolverTotals()
+        check(self.L.ariel_solver_totals(self.h, scene, C.byref(t)), "ariel_solver_totals")
+        return t
+
+    def timer_begin(self):
+        check(self.L.ariel_timer_begin(self.h), "ariel_timer_begin")
+
+    def timer_end(self):
+        ms = C.c_double()
+        check(self.L.ariel_timer_end(self.h, C.byref(ms)), "ariel_timer_end")
+        return ms.value
+
+
+class FlipSim:
+    """FlipSim(maxres, density, stepsize, scene, verbose) -- src/sim/flip.hpp:22-23.
+
+    `scene` is an AsimSceneDesc (the synthetic stand-in for sceneCore::Scene); maxres, density
+    and stepsize override its grid size, lattice density and time step like the reference's
+    constructor arguments do.
+    """
+
+    def __init__(self, maxres, density, stepsize, scene, verbose=False, params=None):
+        desc = A.AsimSceneDesc()
+        C.pointer(desc)[0] = scene
+        desc.dim = int(maxres)
+        desc.density = float(density)
+        desc.stepsize = float(stepsize)
+        self._b = Batch([desc], params)
+        self.m_frame = 0
+        self.verbose = verbose
+
+    def Init(self):
+        """FlipSim::Init (src/sim/flip.cpp:42-77)."""
+        self._b.init()
+        self.m_frame = 0
+
+    def Step(self, saveVDB=False, saveOBJ=False, savePARTIO=False):
+        """FlipSim::Step (src/sim/flip.cpp:92-128).  The export flags are accepted for
+        interface parity; particle export is GetParticles()."""
+        self._b.step(1)
+        self.m_frame += 1
+
+    def GetParticles(self):
+        """FlipSim::GetParticles (src/sim/flip.hpp:29): host copies of the particle state."""
+        return self._b.get_particles(0)
+
+    def GetDimensions(self):
+        """FlipSim::GetDimensions (src/sim/flip.hpp:30)."""
+        n = self._b.dim(0)
+        return (n, n, n)
+
+    def GetScene(self):
+        return self._b.descs[0]
+
+    @property
+    def batch(self):
+        return self._b

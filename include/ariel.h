@@ -1,0 +1,270 @@
+/*
+ * ariel.h -- C ABI of the B200-native FLIP step (sm_100a CUDA behind plain C).
+ *
+ * This library replaces the hot path of betajippity/Ariel, `fluidCore::FlipSim::Step`
+ * (src/sim/flip.cpp:92-128), and the free functions it calls:
+ *   SplatParticlesToMACGrid / SplatMACGridToParticles / EnforceBoundaryVelocity /
+ *   InterpolateVelocity   (src/sim/particlegridoperations.inl:23-29),
+ *   Solve                 (src/sim/solver.inl:23),
+ *   ResampleParticles     (src/sim/particleresampler.inl:23-26),
+ *   ParticleGrid::Sort / MarkCellTypes / BuildSDF (src/grid/particlegrid.hpp:28-39).
+ *
+ * One handle (`ariel_sim`) owns 1..k scenes that are stepped together.  All grid and
+ * particle state stays resident in device memory; the caller owns every host buffer
+ * passed in or out.  Calls on one handle are not thread-safe; distinct handles are.
+ * Every entry point returns an `ariel_status`.
+ *
+ * Units and layouts follow the reference:
+ *   - particle positions are in the unit cube [0,1]^3 (src/grid/macgrid.inl:36-50),
+ *     host particle buffers are xyz-interleaved float triples in particle-id order;
+ *   - grids are cubic, n cells per axis (the reference's G2P assumes a cube:
+ *     src/sim/particlegridoperations.inl:121-124);
+ *   - cell (i,j,k) is stored at (i*n + j)*n + k; the x-face grid has (n+1)*n*n entries at
+ *     (i*n + j)*n + k, the y-face grid n*(n+1)*n at (i*(n+1) + j)*n + k and the z-face
+ *     grid n*n*(n+1) at (i*n + j)*(n+1) + k  (src/grid/macgrid.inl:72-84).
+ */
+#ifndef ARIEL_H
+#define ARIEL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARIEL_ABI_VERSION 1
+
+typedef enum ariel_status {
+    ARIEL_OK = 0,
+    ARIEL_ERR_INVALID_ARG = 1,    /* bad pointer, size, mode or scene index */
+    ARIEL_ERR_OOM = 2,            /* device allocation refused or HBM budget exceeded */
+    ARIEL_ERR_NOT_CONVERGED = 3,  /* pressure solve hit its iteration cap above tolerance */
+    ARIEL_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait ran out (grid barrier, flag) */
+    ARIEL_ERR_CUDA = 5,           /* a CUDA runtime call failed */
+    ARIEL_ERR_STATE = 6,          /* call out of order (e.g. step before init) */
+    ARIEL_ERR_NO_DEVICE = 7,      /* no usable sm_100 device */
+    ARIEL_ERR_NAN = 8             /* non-finite value in host input */
+} ariel_status;
+
+/* Cell types: enum geomtype {SOLID=2, FLUID=1, AIR=0} (src/grid/macgrid.inl:13). */
+enum { ARIEL_AIR = 0, ARIEL_FLUID = 1, ARIEL_SOLID = 2 };
+
+/* Preconditioner.
+ * REF : the reference's BuildPreconditioner/ApplyPreconditioner (src/sim/solver.inl:104-135,
+ *       232-286) including its PRef value==1.0f test (solver.inl:72-78).
+ * MIC0: modified incomplete Cholesky MIC(0) with tau/sigma (Bridson), FP64 factorisation,
+ *       forward/backward substitution as i+j+k wavefront sweeps. */
+enum { ARIEL_PRECOND_REF = 0, ARIEL_PRECOND_MIC0 = 1 };
+
+/* Pressure-solve precision.
+ * REF32: every vector in fp32, the reference's own operator expression (solver.inl:196-230).
+ * FP64 : every PCG vector, coefficient and scalar in fp64 (the plain FP64 GPU path).
+ * MIXED: fp32 SpMV / preconditioner / vector updates inside an fp64 iterative-refinement
+ *        outer loop; fp64 dots, alpha/beta, outer true residual and MIC(0) diagonal. */
+enum { ARIEL_PREC_REF32 = 0, ARIEL_PREC_FP64 = 1, ARIEL_PREC_MIXED = 2 };
+
+/* Stop rule. REF_ABS: r.r <= 1e-2*n^3 (solver.inl:322,339).  REL: |r|/|b| <= tol. */
+enum { ARIEL_STOP_REF_ABS = 0, ARIEL_STOP_REL = 1 };
+
+/* Stages of FlipSim::Step, in call order (src/sim/flip.cpp:92-128).  `ariel_stage` runs one;
+ * `ariel_step` runs all of them and advances the frame counter. */
+enum {
+    ARIEL_STAGE_BEGIN = 0,        /* frame++, AdjustParticlesStuckInSolids, StoreTemp (:93-103) */
+    ARIEL_STAGE_SORT = 1,         /* ParticleGrid::Sort (:104) */
+    ARIEL_STAGE_DENSITY = 2,      /* ComputeDensity (:105) */
+    ARIEL_STAGE_FORCES = 3,       /* ApplyExternalForces (:106) */
+    ARIEL_STAGE_P2G = 4,          /* SplatParticlesToMACGrid (:107) */
+    ARIEL_STAGE_CLASSIFY = 5,     /* MarkCellTypes (:108) + the BuildSDF of Project (:440) */
+    ARIEL_STAGE_BOUNDARY_DIV = 6, /* StorePreviousGrid, EnforceBoundaryVelocity, divergence,
+                                     FlipGrid (:109-110, :420-437, solver.inl:365) */
+    ARIEL_STAGE_SOLVE = 7,        /* BuildPreconditioner + SolveConjugateGradient (solver.inl:356) */
+    ARIEL_STAGE_GRADIENT = 8,     /* SubtractPressureGradient + EnforceBoundaryVelocity (:449,:112) */
+    ARIEL_STAGE_EXTRAPOLATE = 9,  /* ExtrapolateVelocity + SubtractPreviousGrid (:113-114) */
+    ARIEL_STAGE_G2P_ADVECT = 10,  /* SolvePicFlip + AdvectParticles + CheckParticleSolidConstraints
+                                     (:115-118) */
+    ARIEL_STAGE_RESAMPLE = 11,    /* StoreTemp + ResampleParticles + CheckParticleSolidConstraints
+                                     (:119-123) */
+    ARIEL_STAGE_COUNT = 12
+};
+
+/* Grid selectors for ariel_get_grid / ariel_set_grid. */
+enum {
+    ARIEL_GRID_UX = 0, ARIEL_GRID_UY = 1, ARIEL_GRID_UZ = 2,          /* m_mgrid faces, f32 */
+    ARIEL_GRID_PREV_UX = 3, ARIEL_GRID_PREV_UY = 4, ARIEL_GRID_PREV_UZ = 5, /* m_mgrid_previous */
+    ARIEL_GRID_D = 6,   /* divergence (negated after FlipGrid), f32 n^3 */
+    ARIEL_GRID_P = 7,   /* pressure, f32 n^3 */
+    ARIEL_GRID_L = 8,   /* liquid SDF, f32 n^3 */
+    ARIEL_GRID_A = 9,   /* cell types, int32 n^3 */
+    ARIEL_GRID_P64 = 10 /* fp64 pressure kept for FP64/MIXED warm starts, f64 n^3 */
+};
+
+#define ARIEL_MAX_BOXES 8
+#define ARIEL_MAX_SPHERES 8
+#define ARIEL_MAX_FORCES 4
+
+/* Axis-aligned liquid block in unit coordinates (a `mesh_gen` box of the reference's scenes,
+ * src/scene/sceneloader.cpp:346-398), with its starting velocity (scene.cpp:280). */
+typedef struct AsimBox {
+    float lo[3];
+    float hi[3];
+    float vel[3];
+} AsimBox;
+
+/* Static solid sphere in unit coordinates; becomes SOLID particles of mass 10 at the lattice
+ * points inside it (src/scene/scene.cpp:457-477), and the analytic surface for the ray and
+ * point-inside tests of the solid constraints (flip.cpp:130-227). */
+typedef struct AsimSphere {
+    float center[3];
+    float radius;
+} AsimSphere;
+
+typedef struct AsimSceneDesc {
+    int32_t dim;          /* n: cubic grid of n^3 cells (FlipSim maxres) */
+    float density;        /* lattice spacing in cells: 0.5 -> 8 particles/cell (sceneloader.cpp:411) */
+    float stepsize;       /* dt (FlipSim stepsize) */
+    int32_t n_forces;     /* external forces, applied in order (flip.cpp:682-695) */
+    float forces[ARIEL_MAX_FORCES][3];
+    int32_t n_liquid;
+    AsimBox liquid[ARIEL_MAX_BOXES];
+    int32_t n_solid;
+    AsimSphere solid[ARIEL_MAX_SPHERES];
+    uint64_t seed;        /* seeds the in-sub-cell jitter of the initial liquid lattice */
+    float jitter;         /* 1: uniform jitter inside each lattice sub-cell; 0: sub-cell centres */
+    int32_t reserved;
+} AsimSceneDesc;
+
+typedef struct AsimParams {
+    float picflip;            /* FLIP fraction of the PIC/FLIP blend (flip.cpp:27: .95) */
+    int32_t subcell;          /* ghost-fluid pressure boundary (flip.cpp:26: 1) */
+    int32_t precond;          /* ARIEL_PRECOND_* */
+    int32_t precision;        /* ARIEL_PREC_* */
+    int32_t stop_rule;        /* ARIEL_STOP_* */
+    int32_t max_iters;        /* PCG iteration cap; 0 -> n^3 (solver.inl:325) */
+    double tol;               /* relative tolerance for ARIEL_STOP_REL */
+    double inner_tol;         /* MIXED: relative reduction asked of each fp32 inner solve */
+    int32_t max_outer;        /* MIXED: cap on refinement sweeps */
+    int32_t resample_every;   /* resample every k-th step; 1 = every step as the reference
+                                 (flip.cpp:121); 0 = never */
+    double mic_tau;           /* MIC(0) tau (0.97) */
+    double mic_sigma;         /* MIC(0) safety (0.25) */
+    uint64_t rng_seed;        /* counter-based RNG seed for the resampling jitter, which
+                                 replaces rand() (particleresampler.inl:69-71) */
+    int32_t use_graph;        /* capture one step per CUDA graph and replay it */
+    int32_t timing;           /* record per-stage CUDA-event times (adds event records) */
+    double barrier_timeout_ms;/* bound of every device-side spin wait */
+    int32_t fail_on_not_converged; /* return ARIEL_ERR_NOT_CONVERGED from step when a solve
+                                      stops at max_iters above tolerance */
+    int32_t reserved;
+} AsimParams;
+
+typedef struct AsimStats {
+    int64_t frame;            /* FlipSim::m_frame */
+    int64_t n_particles;
+    int64_t n_fluid_cells;    /* FLUID cells at the last solve */
+    int32_t pcg_iterations;   /* last solve: CG iterations (sum of inner iterations for MIXED) */
+    int32_t pcg_outer;        /* last solve: refinement sweeps (MIXED), else 1 */
+    double pcg_rel_residual;  /* last solve: final |r|/|b| (true residual for FP64/MIXED) */
+    double pcg_rr;            /* last solve: final r.r as tested by the stop rule */
+    int32_t pcg_converged;    /* last solve met its stop rule */
+    int32_t precond_exact_path; /* last solve needed the ordered (wavefront) REF preconditioner */
+    double stage_ms[ARIEL_STAGE_COUNT]; /* last step, per stage (when timing is on) */
+    double step_ms;           /* last step, device time (when timing is on) */
+    int32_t last_status;
+    int32_t reserved;
+} AsimStats;
+
+/* Pressure-solve totals accumulated on the device since the last ariel_timing_reset. */
+typedef struct AsimSolverTotals {
+    int64_t solves;
+    int64_t iterations;        /* CG iterations (inner iterations for MIXED) */
+    int64_t outer;             /* refinement sweeps (MIXED), else one per solve */
+    double cell_iterations;    /* sum over solves of FLUID cells x iterations */
+    double cell_outer;         /* sum over solves of FLUID cells x sweeps */
+    int64_t not_converged;
+    int64_t reserved;
+} AsimSolverTotals;
+
+typedef struct ariel_sim ariel_sim;
+
+/* Defaults: the reference's constants, REF preconditioner, REF32 precision, REF_ABS stop. */
+void ariel_params_default(AsimParams* params);
+/* Dam break: liquid block x in [0,.4], y in [0,.6], z in [0,1], gravity -9.8 y, dt 1/240. */
+void ariel_scene_dambreak(AsimSceneDesc* desc, int32_t n);
+const char* ariel_status_string(ariel_status status);
+int32_t ariel_abi_version(void);
+
+/* FlipSim(maxres, density, stepsize, scene, verbose) (src/sim/flip.hpp:22-23). */
+ariel_status ariel_create(const AsimSceneDesc* desc, const AsimParams* params, ariel_sim** out);
+/* k scenes of any sizes stepped together over one packed cell/particle index space. */
+ariel_status ariel_create_batch(const AsimSceneDesc* descs, int32_t k, const AsimParams* params,
+                                ariel_sim** out);
+ariel_status ariel_destroy(ariel_sim* sim);
+ariel_status ariel_scene_count(ariel_sim* sim, int32_t* k);
+
+/* FlipSim::Init (src/sim/flip.cpp:42-77): density normaliser from a 10^3 lattice, particle
+ * seeding (src/scene/scene.cpp:257-360), Sort and MarkCellTypes. */
+ariel_status ariel_init(ariel_sim* sim);
+/* FlipSim::Step (src/sim/flip.cpp:92-128) n times for every scene of the handle. */
+ariel_status ariel_step(ariel_sim* sim, int32_t nsteps);
+/* One stage (ARIEL_STAGE_*) for every scene; does not advance the frame except BEGIN. */
+ariel_status ariel_stage(ariel_sim* sim, int32_t stage);
+ariel_status ariel_synchronize(ariel_sim* sim);
+
+/* FlipSim::GetParticles (src/sim/flip.hpp:29). Any output pointer may be NULL. */
+ariel_status ariel_particle_count(ariel_sim* sim, int32_t scene, int64_t* n);
+ariel_status ariel_get_particles(ariel_sim* sim, int32_t scene, float* pos, float* vel,
+                                 float* density, float* mass, int32_t* type);
+/* Replace a scene's particles (positions/velocities xyz-interleaved, unit coordinates). */
+ariel_status ariel_set_particles(ariel_sim* sim, int32_t scene, int64_t n, const float* pos,
+                                 const float* vel, const float* mass, const int32_t* type);
+/* Particle-to-cell index (per particle, id order) and per-cell counts from the last Sort. */
+ariel_status ariel_get_cells(ariel_sim* sim, int32_t scene, int32_t* particle_cell,
+                             int32_t* cell_count);
+ariel_status ariel_get_grid(ariel_sim* sim, int32_t scene, int32_t which, void* buf,
+                            int64_t nbytes);
+ariel_status ariel_set_grid(ariel_sim* sim, int32_t scene, int32_t which, const void* buf,
+                            int64_t nbytes);
+ariel_status ariel_get_dimensions(ariel_sim* sim, int32_t scene, int32_t* n);
+ariel_status ariel_stats(ariel_sim* sim, int32_t scene, AsimStats* stats);
+/* Normaliser m_max_density computed by Init (flip.cpp:62-70). */
+ariel_status ariel_get_max_density(ariel_sim* sim, int32_t scene, float* max_density);
+
+/* Per-step particle I/O through host buffers (the reference's GetParticles use, with the
+ * particles kept by the caller): xyz-interleaved positions and velocities of the scene's
+ * current particles, in id order.  Upload is asynchronous on the handle's stream (pinned host
+ * memory makes it a true async copy; the buffers must stay valid until the next synchronising
+ * call); download returns when the data is in `pos`/`vel`. */
+ariel_status ariel_upload_state(ariel_sim* sim, int32_t scene, const float* pos, const float* vel);
+ariel_status ariel_download_state(ariel_sim* sim, int32_t scene, float* pos, float* vel);
+
+/* Device timing of whole steps on the handle's stream (CUDA events). */
+ariel_status ariel_timer_begin(ariel_sim* sim);
+ariel_status ariel_timer_end(ariel_sim* sim, double* ms);
+
+/* Per-stage device times accumulated over every step run since the last reset (requires
+ * params.timing = 1, which keeps graph replay and double-buffers the stage events so the
+ * device is never idle while they are read).  ms[ARIEL_STAGE_COUNT] receives the per-stage
+ * sums, solve_kernel_ms the persistent solve kernel alone, step_ms (may be NULL) the
+ * per-step totals of the last `max_steps` steps; *nsteps the number of steps summed. */
+ariel_status ariel_timing_reset(ariel_sim* sim);
+ariel_status ariel_solver_totals(ariel_sim* sim, int32_t scene, AsimSolverTotals* totals);
+ariel_status ariel_timing_get(ariel_sim* sim, double* ms, double* solve_kernel_ms, double* step_ms,
+                              int32_t max_steps, int32_t* nsteps);
+
+/* Device-side failure detection: runs the bounded grid barrier with one arrival missing so
+ * that it must time out after `timeout_ms`; returns ARIEL_ERR_DEVICE_TIMEOUT when the bound
+ * worked and ARIEL_OK if the barrier (wrongly) completed. */
+ariel_status ariel_selftest_barrier_timeout(double timeout_ms);
+
+/* Count of this library's kernel launches issued so far (all handles). */
+int64_t ariel_kernel_launches(void);
+
+/* Text of the last CUDA failure seen by this thread (the failing call and CUDA's message). */
+const char* ariel_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARIEL_H */

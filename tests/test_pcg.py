@@ -1,0 +1,151 @@
+"""Pressure-solve parity: every GPU precision mode against the FP64 CPU oracle.
+
+Inputs are the real divergence / flags / liquid SDF of an evolved dam break, produced by the
+oracle and loaded identically into both sides.  The reported error per solve is
+|P_gpu - P*| / |P*| against a tight (1e-12) FP64 oracle solve P*.
+"""
+import numpy as np
+import pytest
+
+from ariel_b200 import _abi as A
+from ariel_b200.flipsim import Batch
+from oracle.pyoracle import RefSim, apply_fp64, solve_fp64
+
+from helpers import dambreak, evolved_state, params
+
+
+def _solve_inputs(n=24, seed=5, steps=8):
+    desc = dambreak(n, seed=seed)
+    prm = params()
+    st, P, P64 = evolved_state(desc, prm, steps)
+    ora = RefSim(desc, prm)
+    ora.set_particles(st["pos"], st["vel"], st["mass"], st["type"])
+    for g in range(A.STAGE_SOLVE):
+        ora.stage(g)
+    return desc, st, dict(A=ora.get_grid(A.GRID_A), L=ora.get_grid(A.GRID_L), D=ora.get_grid(A.GRID_D),
+                          P=P, P64=P64)
+
+
+def _gpu_solve(desc, st, g, prm):
+    b = Batch([desc], prm)
+    b.set_particles(st["pos"], st["vel"], st["mass"], st["type"])
+    b.set_grid(A.GRID_A, g["A"])
+    b.set_grid(A.GRID_L, g["L"])
+    b.set_grid(A.GRID_D, g["D"])
+    b.set_grid(A.GRID_P, g["P"])
+    b.set_grid(A.GRID_P64, g["P64"])
+    b.stage(A.STAGE_SOLVE)
+    out = dict(P=b.get_grid(A.GRID_P), P64=b.get_grid(A.GRID_P64), stats=b.stats())
+    b.close()
+    return out
+
+
+def _true_rel_residual(n, g, x):
+    fl = g["A"] == A.FLUID
+    b = g["D"].astype(np.float64)
+    ax = apply_fp64(n, g["A"], g["L"], x)
+    r = (b - ax)[fl]
+    return np.linalg.norm(r) / np.linalg.norm(b[fl])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,tol", [(A.PREC_FP64, 1e-5), (A.PREC_FP64, 1e-7), (A.PREC_MIXED, 1e-5),
+                                           (A.PREC_MIXED, 1e-7), (A.PREC_REF32, 1e-5)])
+def test_solve_against_fp64_oracle(precision, tol):
+    n = 24
+    desc, st, g = _solve_inputs(n)
+    fl = g["A"] == A.FLUID
+    xstar, it, rel = solve_fp64(n, g["A"], g["L"], g["D"].astype(np.float64).ravel(), tol=1e-12)
+    assert rel < 1e-10
+    out = _gpu_solve(desc, st, g, params(precision=precision, stop=A.STOP_REL, tol=tol))
+    s = out["stats"]
+    assert s.pcg_converged == 1
+    x = out["P64"] if precision != A.PREC_REF32 else out["P"].astype(np.float64)
+    true_rel = _true_rel_residual(n, g, x)
+    err = np.linalg.norm((x - xstar)[fl]) / np.linalg.norm(xstar[fl])
+    print("precision %d tol %g: iterations %d outer %d true rel residual %.3e error vs FP64 oracle %.3e"
+          % (precision, tol, s.pcg_iterations, s.pcg_outer, true_rel, err))
+    if precision == A.PREC_REF32:
+        assert true_rel < 10 * tol  # fp32 recursive residual drifts from the true one
+    else:
+        assert true_rel <= 1.01 * tol
+    # the solution error is bounded by the residual through the operator's conditioning
+    assert err < 1e3 * tol
+    # non-FLUID pressure is zero (the reference's Op, solver.inl:166-171)
+    assert (out["P"][~fl] == 0).all()
+
+
+def _pocket_grids(n=8):
+    """A FLUID cell X walled by five SOLID cells, whose only FLUID neighbour Y sits above it
+    in k: X's preconditioner value is exactly 1.0f, so the reference's PRef test
+    (solver.inl:74) feeds it into Y's (the ordered path)."""
+    Af = np.zeros((n, n, n), np.int32)
+    L = np.full((n, n, n), 1.6, np.float32)
+    Af[:3, :3, :3] = A.FLUID  # an ordinary liquid block in a corner
+    L[:3, :3, :3] = -0.5
+    X, Y = (5, 5, 4), (5, 5, 5)
+    for c in [(4, 5, 4), (6, 5, 4), (5, 4, 4), (5, 6, 4), (5, 5, 3), (4, 5, 5), (6, 5, 5), (5, 4, 5), (5, 6, 5)]:
+        Af[c] = A.SOLID
+        L[c] = 1.0
+    Af[X] = A.FLUID
+    Af[Y] = A.FLUID
+    L[X] = -0.7
+    L[Y] = -1.0
+    L[5, 5, 6] = 0.5  # AIR above Y: ghost-fluid term 0.5/1.0
+    rng = np.random.default_rng(3)
+    D = rng.standard_normal((n, n, n)).astype(np.float32)
+    return dict(A=Af, L=L, D=D, P=np.zeros((n, n, n), np.float32), P64=np.zeros((n, n, n)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [A.PREC_REF32, A.PREC_FP64])
+def test_pref_quirk_ordered_path(precision):
+    n = 8
+    g = _pocket_grids(n)
+    desc = dambreak(n)
+    # a fixed, small iteration count makes the pressure depend on the preconditioner itself
+    prm = params(precision=precision, stop=A.STOP_REL, tol=1e-14, max_iters=3)
+    ora = RefSim(desc, prm)
+    st = dict(pos=np.array([[0.1, 0.1, 0.1]], np.float32), vel=np.zeros((1, 3), np.float32),
+              mass=np.ones(1, np.float32), type=np.array([A.FLUID], np.int32))
+    ora.set_particles(st["pos"], st["vel"], st["mass"], st["type"])
+    for w, key in [(A.GRID_A, "A"), (A.GRID_L, "L"), (A.GRID_D, "D"), (A.GRID_P, "P"), (A.GRID_P64, "P64")]:
+        ora.set_grid(w, g[key])
+    ora.stage(A.STAGE_SOLVE)
+    out = _gpu_solve(desc, st, g, prm)
+    so = ora.stats()
+    assert so.precond_exact_path == 1 and out["stats"].precond_exact_path == 1
+    assert so.pcg_iterations == out["stats"].pcg_iterations == 3
+    Po = ora.get_grid(A.GRID_P)
+    fl = g["A"] == A.FLUID
+    scale = np.abs(Po[fl]).max()
+    np.testing.assert_allclose(out["P"][fl] / scale, Po[fl] / scale, rtol=0, atol=2e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_mic0_against_oracle(precision):
+    n = 16
+    desc, st, g = _solve_inputs(n, seed=9, steps=5)
+    # MIC(0) after three iterations (FP64 oracle, serial lexicographic factorisation)
+    prm = params(precision=A.PREC_FP64, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-14, max_iters=3)
+    ora = RefSim(desc, prm)
+    ora.set_particles(st["pos"], st["vel"], st["mass"], st["type"])
+    for w, key in [(A.GRID_A, "A"), (A.GRID_L, "L"), (A.GRID_D, "D"), (A.GRID_P, "P"), (A.GRID_P64, "P64")]:
+        ora.set_grid(w, g[key])
+    ora.stage(A.STAGE_SOLVE)
+    fl = g["A"] == A.FLUID
+    if precision == A.PREC_FP64:
+        out = _gpu_solve(desc, st, g, prm)
+        Po = ora.get_grid(A.GRID_P64)
+        scale = np.abs(Po[fl]).max()
+        np.testing.assert_allclose(out["P64"][fl] / scale, Po[fl] / scale, rtol=0, atol=1e-10)
+    # converged MIC(0) solves reach the FP64 oracle's solution and need fewer iterations than
+    # the reference's diagonal preconditioner
+    xstar, _, _ = solve_fp64(n, g["A"], g["L"], g["D"].astype(np.float64).ravel(), tol=1e-12)
+    mic = _gpu_solve(desc, st, g, params(precision=precision, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-7))
+    ref = _gpu_solve(desc, st, g, params(precision=precision, precond=A.PRECOND_REF, stop=A.STOP_REL, tol=1e-7))
+    assert mic["stats"].pcg_converged
+    err = np.linalg.norm((mic["P64"] - xstar)[fl]) / np.linalg.norm(xstar[fl])
+    assert err < 1e-4
+    assert mic["stats"].pcg_iterations < ref["stats"].pcg_iterations
