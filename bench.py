@@ -271,6 +271,7 @@ def main():
     gpu_index = pin_device(local, ws)
     from ariel_b200 import _abi as A
     from ariel_b200.flipsim import Batch
+    from ariel_b200.replicas import aggregate, replica_seed
 
     pg = None
     if ws > 1:
@@ -286,22 +287,13 @@ def main():
         return rc
 
     prec = {"mixed": A.PREC_MIXED, "fp64": A.PREC_FP64, "ref32": A.PREC_REF32}[args.precision]
-    desc = A.scene_dambreak(args.n, seed=1 + rank)
+    desc = A.scene_dambreak(args.n, seed=replica_seed(rank))
     barrier = (lambda: pg.barrier()) if pg else None
     sampler = ClockSampler(gpu_index)
     b, res = run_gpu_pass(A, Batch, desc, make_params(A, prec, args.tol), args.steps, args.warmup, sampler, barrier)
 
-    ms = res["ms"]
     n_local = res["np"]
-    total_particles = n_local
-    if pg:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-        c = torch.tensor([n_local], dtype=torch.float64)
-        pg.all_reduce(c, op=pg.ReduceOp.SUM)
-        total_particles = int(c.item())
+    ms, total_particles = aggregate(res["ms"], n_local, pg)
     value = total_particles * args.steps / (ms / 1000.0)
 
     tim = res["timing"]
@@ -340,12 +332,7 @@ def main():
 
     if not args.no_e2e:
         e2e_ms, h2d, d2h, pinned = run_e2e(b, args.steps)
-        e_ms = e2e_ms
-        if pg:
-            import torch
-            t = torch.tensor([e_ms], dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms, _ = aggregate(e2e_ms, n_local, pg)
         out["e2e"] = {"value": total_particles * args.steps / (e_ms / 1000.0), "unit": "particle-steps/s",
                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "pinned": pinned,
                       "api": "ariel_upload_state + ariel_step + ariel_download_state"}
