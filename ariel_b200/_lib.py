@@ -46,6 +46,7 @@ SIGNATURES = {
     "ariel_selftest_barrier_timeout": ([C.c_double], C.c_int),
     "ariel_kernel_launches": ([], C.c_int64),
     "ariel_last_error": ([], C.c_char_p),
+    "ariel_sort_by_cell_noalloc": ([_vp, C.c_int64, C.c_int32, _vp, _vp, _vp, _vp], C.c_int),
 }
 
 
