@@ -404,7 +404,11 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     A.stop_rule = s->prm.stop_rule;
     A.max_iters = s->prm.max_iters;
     A.max_outer = s->prm.max_outer > 0 ? s->prm.max_outer : 8;
-    A.chunk = 1024;
+    A.chunk = 1024;  // the fast solve kernel's fixed chunk size
+    A.fast = (k <= 128 && A.precond == ARIEL_PRECOND_REF) ? 1 : 0;
+    // the reference preconditioner needs the ordered kernel only in the rare PRef == 1 case,
+    // which only the device knows; keep launching it (it returns at once when not needed)
+    A.may_be_ordered = 1;
     A.tol = s->prm.tol;
     A.inner_tol = s->prm.inner_tol > 0 ? s->prm.inner_tol : 1e-4;
     A.tau = s->prm.mic_tau;
@@ -426,14 +430,21 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     ARIEL_TRY(dalloc(s, &A.pc64, nc));
     ARIEL_TRY(dalloc(s, &A.pc32, nc));
     const size_t vb = s->mode == kFp64 ? 8 : 4;
-    char* v[6];
-    for (int i = 0; i < 6; ++i) ARIEL_TRY(dalloc(s, &v[i], vb * (size_t)nc));
+    char* v[8];
+    for (int i = 0; i < 8; ++i) ARIEL_TRY(dalloc(s, &v[i], vb * (size_t)nc));
     A.r = v[0];
     A.z = v[1];
     A.s0 = v[2];
     A.s1 = v[3];
     A.q = v[4];
     A.ordq = v[5];
+    A.u = v[6];
+    A.p = v[7];
+    char* w4[3];
+    for (int i = 0; i < 3; ++i) ARIEL_TRY(dalloc(s, &w4[i], 4 * vb * (size_t)nc));
+    A.va0 = w4[0];
+    A.va1 = w4[1];
+    A.vb = w4[2];
     if (s->mode == kMixed) {
         ARIEL_TRY(dalloc(s, &A.r64, nc));
         ARIEL_TRY(dalloc(s, &A.d32, nc));
@@ -444,14 +455,14 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
         maxch += (n * n * n + A.chunk - 1) / A.chunk;
     }
     A.max_chunks = std::max(1ll, maxch);
-    ARIEL_TRY(dalloc(s, &A.partial, 2 * A.max_chunks));
+    ARIEL_TRY(dalloc(s, &A.partial, 3 * A.max_chunks));
     ARIEL_TRY(dalloc(s, &A.sc, k));
     ARIEL_TRY(dalloc(s, &A.totals, k));
     ARIEL_CUDA(cudaMemsetAsync(A.totals, 0, sizeof(PcgTotals) * k, s->stream));
     ARIEL_TRY(dalloc(s, &A.ctl, 1));
     ARIEL_TRY(dalloc(s, &A.bar, 1));
     A.S = S;
-    s->pcg_blocks = pcg_max_blocks(s->device, s->mode);
+    s->pcg_blocks = pcg_max_blocks(s->device, s->mode, s->prm.pcg_blocks_per_sm);
     // uploads
     ARIEL_CUDA(cudaMemcpyAsync(s->d_scenes, s->sh.data(), sizeof(SceneDev) * k, cudaMemcpyHostToDevice, s->stream));
     ARIEL_CUDA(cudaMemcpyAsync(s->d_ppref, s->ppref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));

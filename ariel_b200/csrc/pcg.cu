@@ -44,14 +44,18 @@ __device__ __forceinline__ unsigned long long gtimer() {
 // Grid-wide barrier for co-resident blocks.  The last block to arrive runs `leader` (all of its
 // threads) before releasing the others.  Returns false if the wait ran out of time or another
 // block reported an error; the caller must then return.
+// Memory ordering: the block's writes are ordered before its arrival by __syncthreads plus one
+// gpu-scope fence by thread 0 (fences are cumulative); after the release is observed, thread 0
+// fences again (acquire), so every thread of the block may read other blocks' writes with
+// ordinary cached loads after the closing __syncthreads -- the same guarantee grid-wide
+// cooperative-group synchronisation gives.
 template <class F>
 __device__ bool grid_barrier(Barrier* bar, int* dev_error, unsigned long long timeout_ns, F&& leader) {
     __shared__ int s_last, s_ok;
     __shared__ unsigned s_gen;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned g = ld_acquire_u32(&bar->gen);
+        unsigned g = *(volatile unsigned*)&bar->gen;
         s_gen = g;
         __threadfence();
         unsigned arrived = atomicAdd(&bar->count, 1u);
@@ -59,7 +63,7 @@ __device__ bool grid_barrier(Barrier* bar, int* dev_error, unsigned long long ti
         s_ok = 1;
         if (!s_last) {
             unsigned long long t0 = gtimer();
-            while (ld_acquire_u32(&bar->gen) == g) {
+            while (*(volatile unsigned*)&bar->gen == g) {
                 if (*(volatile int*)&bar->error) {
                     s_ok = 0;
                     break;
@@ -70,7 +74,7 @@ __device__ bool grid_barrier(Barrier* bar, int* dev_error, unsigned long long ti
                     s_ok = 0;
                     break;
                 }
-                __nanosleep(32);
+                __nanosleep(20);
             }
         }
         __threadfence();
@@ -78,15 +82,14 @@ __device__ bool grid_barrier(Barrier* bar, int* dev_error, unsigned long long ti
     __syncthreads();
     if (s_last) {
         leader();
-        __threadfence();
         __syncthreads();
         if (threadIdx.x == 0) {
             bar->count = 0;
             __threadfence();
             st_release_u32(&bar->gen, s_gen + 1);
         }
+        __syncthreads();
     }
-    __syncthreads();
     return s_ok != 0;
 }
 
@@ -131,7 +134,7 @@ __device__ __forceinline__ double scene_sum(const double* part, long long b, lon
 #pragma unroll
         for (int u = 0; u < 16; ++u) {
             long long c = base + (long long)u * 32 + lane;
-            x[u] = c < e ? __ldcg(part + c) : 0.0;
+            x[u] = c < e ? part[c] : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < 16; ++u) v += x[u];
@@ -140,13 +143,13 @@ __device__ __forceinline__ double scene_sum(const double* part, long long b, lon
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
-// Whole-struct read of a scene's solver state through L2 (never a possibly stale L1 line).
+// Whole-struct copy of a scene's solver state (read after a grid barrier).
 __device__ __forceinline__ PcgScene load_sc(const PcgScene* p) {
     PcgScene v;
     const int4* src = reinterpret_cast<const int4*>(p);
     int4* dst = reinterpret_cast<int4*>(&v);
 #pragma unroll
-    for (int i = 0; i < (int)(sizeof(PcgScene) / 16); ++i) dst[i] = __ldcg(src + i);
+    for (int i = 0; i < (int)(sizeof(PcgScene) / 16); ++i) dst[i] = src[i];
     return v;
 }
 
@@ -289,9 +292,11 @@ __device__ void hyperplanes(int n, bool reverse, F&& f) {
     }
 }
 
+// Data written by other blocks is read only after a grid barrier (whose acquire makes ordinary
+// loads observe it) or, inside an ordered sweep, after __syncthreads of the writing block.
 template <class T>
 __device__ __forceinline__ T ldv(const T* p) {
-    return __ldcg(p);
+    return *p;
 }
 
 __device__ void ordered_build(const PcgArgs& A, int s) {
@@ -482,7 +487,7 @@ __device__ __forceinline__ T ax_diag(const PcgArgs& A, const SceneDev& D, long l
 // The persistent solve.
 // ------------------------------------------------------------------------------------------
 template <int MODE>
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
+__global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
     using T = typename VT<MODE>::T;
     const DevState& S = A.S;
     const int k = S.k;
@@ -500,12 +505,14 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
     T* r = (T*)A.r;
     T* z = (T*)A.z;
     T* q = (T*)A.q;
-    T* sb[2] = {(T*)A.s0, (T*)A.s1};
+    T* const sb0 = (T*)A.s0;
+    T* const sb1 = (T*)A.s1;
     T* ordq = (T*)A.ordq;
     const T* pcv = MODE == kFp64 ? (const T*)(const void*)A.pc64 : (const T*)(const void*)A.pc32;
     // x of the working solve: P (REF32), P64 (FP64), d32 (MIXED inner correction)
     T* x = MODE == kRef32 ? (T*)(void*)S.P : (MODE == kFp64 ? (T*)(void*)S.P64 : (T*)(void*)A.d32);
-    const bool any_ordered = __ldcg(&A.ctl->any_ordered) != 0;
+    const bool any_ordered = ldv(&A.ctl->any_ordered) != 0;
+    if (A.fast && !any_ordered) return;  // solved by k_pcg_fast
     const unsigned long long tmo = A.timeout_ns;
     __shared__ int s_active;
 
@@ -527,7 +534,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
     // ---- Phase 0: ordered preconditioner build -------------------------------------------
     if (any_ordered) {
         for (int s = blockIdx.x; s < k; s += gridDim.x)
-            if (__ldcg(&SC[s].ordered)) ordered_build(A, s);
+            if (ldv(&SC[s].ordered)) ordered_build(A, s);
         if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
     }
 
@@ -540,7 +547,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
             chunk_range(ch, s, t0, t1);
             const SceneDev& D = S.scenes[s];
             double a0 = 0.0, a1 = 0.0;
-            if (!__ldcg(&SC[s].done)) {
+            if (!ldv(&SC[s].done)) {
                 for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                     long long c = A.fl[t];
                     double bv = (double)S.D[c];
@@ -620,15 +627,183 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
             }
         });
         if (!ok) return;
-        if (__ldcg(&A.ctl->all_done)) break;
+        if (ldv(&A.ctl->all_done)) break;
+
+        if (MODE != kRef32 && !any_ordered) {
+            // ---- single-reduction PCG (Chronopoulos & Gear, 1989): one grid barrier per
+            // iteration.  Iteration i reads r_i = rb[i&1], w_i = wb[i&1], s_{i-1} = sb[(i+1)&1],
+            // u_i, p_{i-1}, x_i and writes s_i = w_i + beta s_{i-1} (sb[i&1]), p_i = u_i + beta
+            // p_{i-1}, x_{i+1} = x_i + alpha p_i, r_{i+1} = r_i - alpha s_i (rb[(i+1)&1]),
+            // u_{i+1} = M r_{i+1}, w_{i+1} = A u_{i+1} (wb[(i+1)&1]).  The neighbour values of
+            // u_{i+1} that A needs are recomputed from the same old arrays, bit-identically to
+            // what their owners write.
+            T* const rb0 = r;
+            T* const rb1 = ordq;
+            T* const wb0 = z;
+            T* const wb1 = q;
+            T* u = (T*)A.u;
+            T* pv = (T*)A.p;
+            double* part2 = A.partial + 2 * MC;
+            auto precond = [&](long long c, T rv) -> T { return (rv * ldv(pcv + c)) * ldv(pcv + c); };
+            auto write_part3 = [&](long long ch, double a, double b, double c3) {
+                double z3 = 0.0;
+                block_sum2(a, b);
+                block_sum2(c3, z3);
+                if (threadIdx.x == 0) {
+                    part0[ch] = a;
+                    part1[ch] = b;
+                    part2[ch] = c3;
+                }
+            };
+            // Phase I1: r_0 (MIXED: from r64), u_0 = M r_0, w_0 = A u_0, (r,u), (w,u), (r,r)
+            for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                int s;
+                long long t0, t1;
+                chunk_range(ch, s, t0, t1);
+                const SceneDev& D = S.scenes[s];
+                double g0 = 0.0, d0 = 0.0, q0 = 0.0;
+                if (!ldv(&SC[s].inner_done)) {
+                    auto r0 = [&](long long qq) -> T { return MODE == kMixed ? (T)A.r64[qq] : ldv(r + qq); };
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = A.fl[t];
+                        T rv = r0(c);
+                        T uv = precond(c, rv);
+                        T wv = ax_diag<T>(A, D, c, uv, [&](long long qq) { return precond(qq, r0(qq)); });
+                        if (MODE == kMixed) {
+                            rb0[c] = rv;
+                            x[c] = (T)0;
+                        }
+                        u[c] = uv;
+                        wb0[c] = wv;
+                        g0 += (double)rv * (double)uv;
+                        d0 += (double)wv * (double)uv;
+                        q0 += (double)rv * (double)rv;
+                    }
+                }
+                write_part3(ch, g0, d0, q0);
+            }
+            ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+                const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+                for (int s = wid; s < k; s += blockDim.x / 32) {
+                    double g = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                    double d = scene_sum(part1, ch_s[s], ch_s[s + 1]);
+                    if (lane == 0) {
+                        PcgScene P = load_sc(SC + s);
+                        if (!P.inner_done) {
+                            P.rho = g;
+                            P.alpha = d != 0.0 ? g / d : 0.0;
+                            P.beta = 0.0;
+                            SC[s] = P;
+                        }
+                    }
+                }
+            });
+            if (!ok) return;
+            for (int it = 0;; ++it) {
+                const int cur = it & 1, nxt = cur ^ 1;
+                for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                    int s;
+                    long long t0, t1;
+                    chunk_range(ch, s, t0, t1);
+                    const SceneDev& D = S.scenes[s];
+                    double g1 = 0.0, d1 = 0.0, q1 = 0.0;
+                    if (!ldv(&SC[s].inner_done)) {
+                        const T al = (T)ldv(&SC[s].alpha);
+                        const T bt = (T)ldv(&SC[s].beta);
+                        const T* rc = cur ? rb1 : rb0;
+                        const T* wc = cur ? wb1 : wb0;
+                        const T* sp = nxt ? sb1 : sb0;
+                        T* sw = cur ? sb1 : sb0;
+                        T* rw = nxt ? rb1 : rb0;
+                        T* ww = nxt ? wb1 : wb0;
+                        // s_i at any FLUID cell, and u_{i+1} = M (r_i - alpha s_i) there
+                        auto s_i = [&](long long qq) -> T { return it == 0 ? ldv(wc + qq) : ldv(wc + qq) + bt * ldv(sp + qq); };
+                        auto u_n = [&](long long qq) -> T { return precond(qq, ldv(rc + qq) - al * s_i(qq)); };
+                        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                            long long c = A.fl[t];
+                            T sv = s_i(c);
+                            T pvv = it == 0 ? ldv(u + c) : ldv(u + c) + bt * ldv(pv + c);
+                            T xv = ldv(x + c) + al * pvv;
+                            T rn = ldv(rc + c) - al * sv;
+                            T un = precond(c, rn);
+                            T wn = ax_diag<T>(A, D, c, un, u_n);
+                            sw[c] = sv;
+                            pv[c] = pvv;
+                            x[c] = xv;
+                            rw[c] = rn;
+                            u[c] = un;
+                            ww[c] = wn;
+                            g1 += (double)rn * (double)un;
+                            d1 += (double)wn * (double)un;
+                            q1 += (double)rn * (double)rn;
+                        }
+                    }
+                    write_part3(ch, g1, d1, q1);
+                }
+                ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
+                    if (threadIdx.x == 0) s_active = 0;
+                    __syncthreads();
+                    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+                    for (int s = wid; s < k; s += blockDim.x / 32) {
+                        double g = scene_sum(part0, ch_s[s], ch_s[s + 1]);
+                        double d = scene_sum(part1, ch_s[s], ch_s[s + 1]);
+                        double rr = scene_sum(part2, ch_s[s], ch_s[s + 1]);
+                        if (lane == 0) {
+                            PcgScene P = load_sc(SC + s);
+                            if (!P.inner_done) {
+                                const int n = S.scenes[s].n;
+                                P.iters += 1;
+                                P.rr = rr;
+                                const int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+                                bool conv = rr <= P.target;
+                                if (conv || P.iters >= cap) {
+                                    P.inner_done = 1;
+                                    if (MODE != kMixed) {
+                                        P.done = 1;
+                                        P.converged = conv;
+                                    }
+                                } else {
+                                    double beta = P.rho != 0.0 ? g / P.rho : 0.0;
+                                    double den = d - (P.alpha != 0.0 ? beta * g / P.alpha : 0.0);
+                                    P.beta = beta;
+                                    P.alpha = den != 0.0 ? g / den : 0.0;
+                                    P.rho = g;
+                                    atomicAdd(&s_active, 1);
+                                }
+                                SC[s] = P;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    if (threadIdx.x == 0) A.ctl->all_inner_done = s_active == 0;
+                });
+                if (!ok) return;
+                if (ldv(&A.ctl->all_inner_done)) break;
+            }
+            // the solution of this (inner) solve is x; MIXED folds it into x64 below
+            if (MODE != kMixed) break;
+            for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                int s;
+                long long t0, t1;
+                chunk_range(ch, s, t0, t1);
+                if (ldv(&SC[s].done)) continue;
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = A.fl[t];
+                    S.P64[c] = ldv(S.P64 + c) + (double)ldv(x + c);
+                }
+            }
+            if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
+            ++outer;
+            continue;
+        }
 
         // ---- Phase I: z = M r, s = z, rho = z.r (MIXED: r32 = r64, d = 0) ------------------
         for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
             int s;
             long long t0, t1;
             chunk_range(ch, s, t0, t1);
-            const bool active = !__ldcg(&SC[s].inner_done);
-            const bool ord = __ldcg(&SC[s].ordered) != 0;
+            const bool active = !ldv(&SC[s].inner_done);
+            const bool ord = ldv(&SC[s].ordered) != 0;
             double a0 = 0.0;
             if (active) {
                 for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
@@ -644,7 +819,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                     if (!ord) {
                         T zv = precond_elem(c, rv);
                         z[c] = zv;
-                        sb[0][c] = zv;
+                        sb0[c] = zv;
                         a0 += (double)zv * (double)rv;
                     }
                 }
@@ -654,13 +829,13 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
         if (any_ordered) {
             if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
             for (int s = blockIdx.x; s < k; s += gridDim.x) {
-                if (!__ldcg(&SC[s].ordered) || __ldcg(&SC[s].inner_done)) continue;
+                if (!ldv(&SC[s].ordered) || ldv(&SC[s].inner_done)) continue;
                 ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
                 double a0 = 0.0;
                 for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
                     long long c = A.fl[t];
                     T zv = ldv(z + c);
-                    sb[0][c] = zv;
+                    sb0[c] = zv;
                     a0 += (double)zv * (double)ldv(r + c);
                 }
                 double b0 = 0.0;
@@ -690,8 +865,8 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
 
         // ---- CG iterations -------------------------------------------------------------------
         for (int it = 0;; ++it) {
-            T* s_cur = sb[it & 1];
-            T* s_prev = sb[(it + 1) & 1];
+            T* s_cur = (it & 1) ? sb1 : sb0;
+            T* s_prev = (it & 1) ? sb0 : sb1;
             // Phase A: s = z + beta s (it > 0), q = A s, s.q
             for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
                 int s;
@@ -699,9 +874,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                 chunk_range(ch, s, t0, t1);
                 const SceneDev& D = S.scenes[s];
                 double a0 = 0.0;
-                if (!__ldcg(&SC[s].inner_done)) {
-                    const double beta = __ldcg(&SC[s].beta);
-                    const float beta32 = __ldcg(&SC[s].beta32);
+                if (!ldv(&SC[s].inner_done)) {
+                    const double beta = ldv(&SC[s].beta);
+                    const float beta32 = ldv(&SC[s].beta32);
                     const T bt = MODE == kRef32 ? (T)beta32 : (T)beta;
                     auto sval = [&](long long qq) -> T {
                         if (it == 0) return ldv(s_cur + qq);
@@ -745,8 +920,8 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                 long long t0, t1;
                 chunk_range(ch, s, t0, t1);
                 double a0 = 0.0, a1 = 0.0;
-                if (!__ldcg(&SC[s].inner_done)) {
-                    const T al = MODE == kRef32 ? (T)__ldcg(&SC[s].alpha32) : (T)__ldcg(&SC[s].alpha);
+                if (!ldv(&SC[s].inner_done)) {
+                    const T al = MODE == kRef32 ? (T)ldv(&SC[s].alpha32) : (T)ldv(&SC[s].alpha);
                     const bool fuse = !any_ordered;
                     for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                         long long c = A.fl[t];
@@ -772,9 +947,9 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                     int s;
                     long long t0, t1;
                     chunk_range(ch, s, t0, t1);
-                    if (__ldcg(&SC[s].ordered)) continue;
+                    if (ldv(&SC[s].ordered)) continue;
                     double a1 = 0.0;
-                    if (!__ldcg(&SC[s].inner_done)) {
+                    if (!ldv(&SC[s].inner_done)) {
                         for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                             long long c = A.fl[t];
                             T rv = ldv(r + c);
@@ -788,7 +963,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                     if (threadIdx.x == 0) part1[ch] = a1;
                 }
                 for (int s = blockIdx.x; s < k; s += gridDim.x) {
-                    if (!__ldcg(&SC[s].ordered) || __ldcg(&SC[s].inner_done)) continue;
+                    if (!ldv(&SC[s].ordered) || ldv(&SC[s].inner_done)) continue;
                     ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
                     double a1 = 0.0;
                     for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
@@ -838,7 +1013,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
                 if (threadIdx.x == 0) A.ctl->all_inner_done = s_active == 0;
             });
             if (!ok) return;
-            if (__ldcg(&A.ctl->all_inner_done)) break;
+            if (ldv(&A.ctl->all_inner_done)) break;
         }
 
         if (MODE != kMixed) break;
@@ -847,7 +1022,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs A) {
             int s;
             long long t0, t1;
             chunk_range(ch, s, t0, t1);
-            if (__ldcg(&SC[s].done)) continue;
+            if (ldv(&SC[s].done)) continue;
             for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                 long long c = A.fl[t];
                 S.P64[c] = ldv(S.P64 + c) + (double)ldv(x + c);
@@ -925,6 +1100,595 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
     return cudaGetLastError();
 }
 
+// ==========================================================================================
+// Fast path (elementwise reference preconditioner, up to kFastMaxScenes scenes per launch).
+//
+// No leader block: a grid barrier is a monotonic arrival counter (barrier e completes when it
+// reaches e * gridDim.x), after which every block reads all chunk partials and reduces each
+// scene's range in the same fixed tree.  Every block therefore holds bit-identical copies of
+// every scene's alpha/beta/stop state in shared memory, and a barrier costs one arrival plus
+// one partial read on the critical path.  Each block also keeps the FLUID-cell indices of its
+// first chunks in shared memory for the whole solve.
+// ==========================================================================================
+constexpr int kFastMaxScenes = 128;
+constexpr int kChunkCells = 1024;
+constexpr int kFlCacheChunks = 4;
+
+struct SceneLocal {
+    double bb, rr, rho, alpha, beta, target, rr_out;
+    float alpha32, beta32, rho32;
+    int iters, outer, done, inner_done, converged, nf;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_cnt(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Barrier number `epoch` (1, 2, ...) of this launch.  Same ordering argument as grid_barrier.
+__device__ bool count_barrier(Barrier* bar, int* dev_error, unsigned epoch, unsigned long long timeout_ns) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        __threadfence();
+        atomicAdd(&bar->count, 1u);
+        const unsigned target = epoch * gridDim.x;
+        const unsigned long long t0 = gtimer();
+        while (ld_acquire_cnt(&bar->count) < target) {
+            if (*(volatile int*)&bar->error) {
+                s_ok = 0;
+                break;
+            }
+            if (gtimer() - t0 > timeout_ns) {
+                atomicExch(&bar->error, 1);
+                if (dev_error) atomicExch(dev_error, 1);
+                s_ok = 0;
+                break;
+            }
+            __nanosleep(16);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Sums of three partial arrays over [b, e) by one warp (fixed tree depending only on e - b).
+__device__ __forceinline__ void scene_sum3(const double* p0, const double* p1, const double* p2, int nsum,
+                                           long long b, long long e, double& o0, double& o1, double& o2) {
+    const int lane = threadIdx.x & 31;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    for (long long base = b; base < e; base += 32 * 16) {
+        double x0[16], x1[16], x2[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            long long c = base + (long long)u * 32 + lane;
+            bool in = c < e;
+            x0[u] = in ? p0[c] : 0.0;
+            x1[u] = (in && nsum > 1) ? p1[c] : 0.0;
+            x2[u] = (in && nsum > 2) ? p2[c] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            v0 += x0[u];
+            v1 += x1[u];
+            v2 += x2[u];
+        }
+    }
+    v0 = warp_sum(v0);
+    v1 = warp_sum(v1);
+    v2 = warp_sum(v2);
+    o0 = __shfl_sync(0xffffffffu, v0, 0);
+    o1 = __shfl_sync(0xffffffffu, v1, 0);
+    o2 = __shfl_sync(0xffffffffu, v2, 0);
+}
+
+// Packed per-cell state of the single-reduction path (T = float for MIXED, double for FP64):
+//   Av[parity][c] = (r_i, w_i, s_{i-1}, pc)  -- read at c and its six neighbours, so
+//                                              double-buffered by iteration parity;
+//   Bv[c]         = (u_i, p_{i-1}, x_i, -)   -- read and written only by c's owner.
+template <class T>
+struct V4;
+template <>
+struct V4<float> {
+    using type = float4;
+};
+template <>
+struct V4<double> {
+    using type = double4;
+};
+__device__ __forceinline__ double4 ld4(const double4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = q[0], b = q[1];
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld4(const float4* p) { return *p; }
+__device__ __forceinline__ void st4(double4* p, double4 v) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[0] = make_double2(v.x, v.y);
+    q[1] = make_double2(v.z, v.w);
+}
+__device__ __forceinline__ void st4(float4* p, float4 v) { *p = v; }
+template <class T>
+__device__ __forceinline__ typename V4<T>::type mk4(T a, T b, T c, T d);
+template <>
+__device__ __forceinline__ float4 mk4<float>(float a, float b, float c, float d) {
+    return make_float4(a, b, c, d);
+}
+template <>
+__device__ __forceinline__ double4 mk4<double>(double a, double b, double c, double d) {
+    return make_double4(a, b, c, d);
+}
+
+size_t fast_dyn_smem(int mode) {
+    const size_t tb = mode == kFp64 ? 8 : 4;
+    return (size_t)kFlCacheChunks * kChunkCells * (4 + 1 + tb);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
+    using T = typename VT<MODE>::T;
+    using T4 = typename V4<T>::type;
+    if (A.ctl->any_ordered) return;  // the ordered preconditioner runs in k_pcg
+    const DevState& S = A.S;
+    const int k = S.k;
+    __shared__ long long fl_s[kFastMaxScenes + 1], ch_s[kFastMaxScenes + 1];
+    __shared__ SceneLocal L[kFastMaxScenes];
+    __shared__ int s_active;
+    // per-solve caches of this block's first kFlCacheChunks chunks: FLUID cell index,
+    // neighbour mask, diagonal
+    extern __shared__ __align__(16) unsigned char dyn[];
+    T* dgc = reinterpret_cast<T*>(dyn);
+    uint32_t* flc = reinterpret_cast<uint32_t*>(dyn + sizeof(T) * kFlCacheChunks * kChunkCells);
+    uint8_t* mkc = reinterpret_cast<uint8_t*>(flc + kFlCacheChunks * kChunkCells);
+    for (int i = threadIdx.x; i <= k; i += blockDim.x) {
+        fl_s[i] = A.fl_pref[i];
+        ch_s[i] = A.ch_pref[i];
+    }
+    for (int i = threadIdx.x; i < k; i += blockDim.x) {
+        SceneLocal z{};
+        z.nf = A.sc[i].nf;
+        L[i] = z;
+    }
+    __syncthreads();
+    const long long nch = ch_s[k];
+    const long long MC = A.max_chunks;
+    double* part0 = A.partial;
+    double* part1 = A.partial + MC;
+    double* part2 = A.partial + 2 * MC;
+    const unsigned long long tmo = A.timeout_ns;
+    unsigned epoch = 0;
+    auto chunk_of = [&](int j, int& s, long long& t0, long long& t1) -> bool {
+        long long ch = blockIdx.x + (long long)j * gridDim.x;
+        if (ch >= nch) return false;
+        s = find_scene(ch_s, k, ch);
+        t0 = fl_s[s] + (ch - ch_s[s]) * kChunkCells;
+        t1 = min(t0 + (long long)kChunkCells, fl_s[s + 1]);
+        return true;
+    };
+    for (int j = 0; j < kFlCacheChunks; ++j) {
+        int s;
+        long long t0, t1;
+        if (!chunk_of(j, s, t0, t1)) break;
+        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+            uint32_t c = A.fl[t];
+            int o = j * kChunkCells + (int)(t - t0);
+            flc[o] = c;
+            mkc[o] = A.mask[c];
+            dgc[o] = (T)A.diag[c];
+        }
+    }
+    __syncthreads();
+    auto cell_at = [&](int j, long long t, long long t0) -> long long {
+        return j < kFlCacheChunks ? (long long)flc[j * kChunkCells + (int)(t - t0)] : (long long)A.fl[t];
+    };
+    auto mask_at = [&](int j, long long t, long long t0, long long c) -> uint32_t {
+        return j < kFlCacheChunks ? (uint32_t)mkc[j * kChunkCells + (int)(t - t0)] : (uint32_t)A.mask[c];
+    };
+    auto diag_at = [&](int j, long long t, long long t0, long long c) -> T {
+        return j < kFlCacheChunks ? dgc[j * kChunkCells + (int)(t - t0)] : (T)A.diag[c];
+    };
+    auto put3 = [&](int j, double a, double b, double c) {
+        double z0 = 0.0;
+        block_sum2(a, b);
+        block_sum2(c, z0);
+        if (threadIdx.x == 0) {
+            long long ch = blockIdx.x + (long long)j * gridDim.x;
+            part0[ch] = a;
+            part1[ch] = b;
+            part2[ch] = c;
+        }
+    };
+    auto reduce = [&](int nsum, auto&& f) {
+        if (threadIdx.x == 0) s_active = 0;
+        __syncthreads();
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int s = wid; s < k; s += blockDim.x / 32) {
+            if (L[s].inner_done && L[s].done) continue;
+            double v0, v1, v2;
+            scene_sum3(part0, part1, part2, nsum, ch_s[s], ch_s[s + 1], v0, v1, v2);
+            if (lane == 0) {
+                if (f(s, L[s], v0, v1, v2)) atomicAdd(&s_active, 1);
+            }
+        }
+        __syncthreads();
+        return s_active;
+    };
+
+    T* r = (T*)A.r;
+    T* z = (T*)A.z;
+    T* q = (T*)A.q;
+    T* const sb0 = (T*)A.s0;
+    T* const sb1 = (T*)A.s1;
+    const T* pcv = MODE == kFp64 ? (const T*)(const void*)A.pc64 : (const T*)(const void*)A.pc32;
+    T* x = MODE == kRef32 ? (T*)(void*)S.P : (MODE == kFp64 ? (T*)(void*)S.P64 : (T*)(void*)A.d32);
+    auto precond = [&](long long c, T rv) -> T { return (rv * pcv[c]) * pcv[c]; };
+    T4* const Av0 = (T4*)A.va0;
+    T4* const Av1 = (T4*)A.va1;
+    T4* const Bv = (T4*)A.vb;
+
+    int outer = 0;
+    while (true) {
+        // ---- residual r = b - A x, |b|^2 --------------------------------------------------
+        for (int j = 0;; ++j) {
+            int s;
+            long long t0, t1;
+            if (!chunk_of(j, s, t0, t1)) break;
+            const SceneDev& D = S.scenes[s];
+            double a0 = 0.0, a1 = 0.0;
+            if (!L[s].done) {
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = cell_at(j, t, t0);
+                    double bv = (double)S.D[c];
+                    if (MODE == kRef32) {
+                        float xc = S.P[c];
+                        float ax = ax_ref32(S, D, c, xc, [&](long long qq) { return S.P[qq]; });
+                        float rv = S.D[c] + (-1.0f) * ax;
+                        r[c] = (T)rv;
+                        a0 += (double)rv * (double)rv;
+                    } else {
+                        double xc = S.P64[c];
+                        double ax = ax_diag<double>(A, D, c, xc, [&](long long qq) { return S.P64[qq]; });
+                        double rv = bv - ax;
+                        if (MODE == kMixed)
+                            A.r64[c] = rv;
+                        else
+                            r[c] = (T)rv;
+                        a0 += rv * rv;
+                    }
+                    a1 += bv * bv;
+                }
+            }
+            put3(j, a0, a1, 0.0);
+        }
+        if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+        int active = reduce(2, [&](int s, SceneLocal& P, double rr, double bb, double) -> bool {
+            if (P.done) return false;
+            const int n = S.scenes[s].n;
+            if (outer == 0) P.bb = bb;
+            P.rr_out = rr;
+            if (MODE == kMixed) P.outer += 1;
+            double lim2 = A.tol * A.tol * P.bb;
+            double abs_eps = (double)(1.0e-2f * (float)(n * n * n));
+            bool conv = false;
+            if (A.stop_rule == ARIEL_STOP_REL)
+                conv = rr <= lim2;
+            else if (MODE == kMixed)
+                conv = outer > 0 && rr <= abs_eps;
+            if (P.nf == 0) conv = true;
+            int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+            if (conv) {
+                P.done = 1;
+                P.converged = 1;
+            } else if (MODE == kMixed && (P.outer > A.max_outer || P.iters >= cap)) {
+                P.done = 1;
+                P.converged = 0;
+            }
+            if (P.done) {
+                P.inner_done = 1;
+                return false;
+            }
+            P.inner_done = 0;
+            P.rr = rr;
+            if (MODE == kMixed) {
+                double a = A.inner_tol * A.inner_tol * rr;
+                double b = A.stop_rule == ARIEL_STOP_REL ? 0.25 * lim2 : 0.0;
+                P.target = a > b ? a : b;
+            } else {
+                P.target = A.stop_rule == ARIEL_STOP_REL ? lim2 : abs_eps;
+            }
+            return true;
+        });
+        if (active == 0) break;
+
+        if (MODE != kRef32) {
+            // ---- single-reduction PCG (Chronopoulos & Gear, 1989), one barrier per
+            // iteration.  Iteration i reads Av[i&1] = (r_i, w_i, s_{i-1}, pc) at c and its
+            // neighbours and Bv = (u_i, p_{i-1}, x_i) at c, and writes s_i = w_i + beta s_{i-1},
+            // p_i = u_i + beta p_{i-1}, x_{i+1} = x_i + alpha p_i, r_{i+1} = r_i - alpha s_i,
+            // u_{i+1} = M r_{i+1} and w_{i+1} = A u_{i+1}; the neighbour values of u_{i+1} are
+            // recomputed from the same old state, bit-identically to what their owners write.
+            for (int j = 0;; ++j) {
+                int s;
+                long long t0, t1;
+                if (!chunk_of(j, s, t0, t1)) break;
+                const SceneDev& D = S.scenes[s];
+                double g0 = 0.0, d0 = 0.0, q0 = 0.0;
+                if (!L[s].inner_done) {
+                    auto r0 = [&](long long qq) -> T { return MODE == kMixed ? (T)A.r64[qq] : r[qq]; };
+                    const T scale = (T)(1.0 / (double)D.ax_h);
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = cell_at(j, t, t0);
+                        const uint32_t m = mask_at(j, t, t0, c);
+                        T rv = r0(c);
+                        T pcc = pcv[c];
+                        T uv = (rv * pcc) * pcc;
+                        T acc = diag_at(j, t, t0, c) * uv;
+#pragma unroll
+                        for (int d = 0; d < 6; ++d)
+                            if (m & (1u << d)) {
+                                long long qq = c + nb_off(d, D.n);
+                                acc -= precond(qq, r0(qq));
+                            }
+                        T wv = acc * scale;
+                        T xv = MODE == kMixed ? (T)0 : S.P64[c];
+                        st4(Av0 + c, mk4<T>(rv, wv, (T)0, pcc));
+                        st4(Bv + c, mk4<T>(uv, (T)0, xv, (T)0));
+                        g0 += (double)rv * (double)uv;
+                        d0 += (double)wv * (double)uv;
+                        q0 += (double)rv * (double)rv;
+                    }
+                }
+                put3(j, g0, d0, q0);
+            }
+            if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+            reduce(2, [&](int, SceneLocal& P, double g, double d, double) -> bool {
+                if (P.inner_done) return false;
+                P.rho = g;
+                P.alpha = d != 0.0 ? g / d : 0.0;
+                P.beta = 0.0;
+                return true;
+            });
+            for (int it = 0;; ++it) {
+                const T4* Ac = (it & 1) ? Av1 : Av0;
+                T4* An = (it & 1) ? Av0 : Av1;
+                for (int j = 0;; ++j) {
+                    int s;
+                    long long t0, t1;
+                    if (!chunk_of(j, s, t0, t1)) break;
+                    const SceneDev& D = S.scenes[s];
+                    double g1 = 0.0, d1 = 0.0, q1 = 0.0;
+                    if (!L[s].inner_done) {
+                        const T al = (T)L[s].alpha;
+                        const T bt = (T)L[s].beta;
+                        const T scale = (T)(1.0 / (double)D.ax_h);
+                        const long long nn = (long long)D.n * D.n, n1 = D.n;
+                        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                            const long long c = cell_at(j, t, t0);
+                            const uint32_t m = mask_at(j, t, t0, c);
+                            const T dg = diag_at(j, t, t0, c);
+                            // all loads first: own state and the six neighbours' (r, w, s, pc)
+                            const T4 a = ld4(Ac + c);
+                            const T4 b = ld4(Bv + c);
+                            T4 nb[6];
+                            const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
+#pragma unroll
+                            for (int d = 0; d < 6; ++d) nb[d] = ld4(Ac + ((m >> d) & 1u ? c + off[d] : c));
+                            const T sv = it == 0 ? a.y : a.y + bt * a.z;
+                            const T pvv = it == 0 ? b.x : b.x + bt * b.y;
+                            const T xv = b.z + al * pvv;
+                            const T rn = a.x - al * sv;
+                            const T un = (rn * a.w) * a.w;
+                            T acc = dg * un;
+#pragma unroll
+                            for (int d = 0; d < 6; ++d) {
+                                if ((m >> d) & 1u) {
+                                    const T4 e = nb[d];
+                                    const T sq = it == 0 ? e.y : e.y + bt * e.z;
+                                    const T rq = e.x - al * sq;
+                                    acc -= (rq * e.w) * e.w;
+                                }
+                            }
+                            const T wn = acc * scale;
+                            st4(An + c, mk4<T>(rn, wn, sv, a.w));
+                            st4(Bv + c, mk4<T>(un, pvv, xv, (T)0));
+                            g1 += (double)rn * (double)un;
+                            d1 += (double)wn * (double)un;
+                            q1 += (double)rn * (double)rn;
+                        }
+                    }
+                    put3(j, g1, d1, q1);
+                }
+                if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+                int act = reduce(3, [&](int s, SceneLocal& P, double g, double d, double rr) -> bool {
+                    if (P.inner_done) return false;
+                    const int n = S.scenes[s].n;
+                    P.iters += 1;
+                    P.rr = rr;
+                    const int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+                    bool conv = rr <= P.target;
+                    if (conv || P.iters >= cap) {
+                        P.inner_done = 1;
+                        if (MODE != kMixed) {
+                            P.done = 1;
+                            P.converged = conv;
+                        }
+                        return false;
+                    }
+                    double beta = P.rho != 0.0 ? g / P.rho : 0.0;
+                    double den = d - (P.alpha != 0.0 ? beta * g / P.alpha : 0.0);
+                    P.beta = beta;
+                    P.alpha = den != 0.0 ? g / den : 0.0;
+                    P.rho = g;
+                    return true;
+                });
+                if (act == 0) break;
+            }
+            // fold the solve's x back: MIXED adds the correction to x64, FP64 stores x64
+            for (int j = 0;; ++j) {
+                int s;
+                long long t0, t1;
+                if (!chunk_of(j, s, t0, t1)) break;
+                if (MODE == kMixed && L[s].done) continue;
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = cell_at(j, t, t0);
+                    const T4 b = ld4(Bv + c);
+                    S.P64[c] = MODE == kMixed ? S.P64[c] + (double)b.z : (double)b.z;
+                }
+            }
+            if (MODE != kMixed) break;
+            if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+            ++outer;
+            continue;
+        }
+
+        // ---- REF32: the reference's two-reduction PCG (solver.inl:289-354) ------------------
+        for (int j = 0;; ++j) {
+            int s;
+            long long t0, t1;
+            if (!chunk_of(j, s, t0, t1)) break;
+            double a0 = 0.0;
+            if (!L[s].inner_done) {
+                for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                    long long c = cell_at(j, t, t0);
+                    T rv = r[c];
+                    T zv = precond(c, rv);
+                    z[c] = zv;
+                    sb0[c] = zv;
+                    a0 += (double)zv * (double)rv;
+                }
+            }
+            put3(j, a0, 0.0, 0.0);
+        }
+        if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+        reduce(1, [&](int, SceneLocal& P, double rho, double, double) -> bool {
+            if (P.inner_done) return false;
+            P.rho = rho;
+            P.rho32 = (float)rho;
+            return true;
+        });
+        for (int it = 0;; ++it) {
+            T* s_cur = (it & 1) ? sb1 : sb0;
+            T* s_prev = (it & 1) ? sb0 : sb1;
+            for (int j = 0;; ++j) {
+                int s;
+                long long t0, t1;
+                if (!chunk_of(j, s, t0, t1)) break;
+                const SceneDev& D = S.scenes[s];
+                double a0 = 0.0;
+                if (!L[s].inner_done) {
+                    const T bt = (T)L[s].beta32;
+                    auto sval = [&](long long qq) -> T { return it == 0 ? s_cur[qq] : z[qq] + bt * s_prev[qq]; };
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = cell_at(j, t, t0);
+                        T sc_ = sval(c);
+                        if (it > 0) s_cur[c] = sc_;
+                        T qv = ax_ref32(S, D, c, sc_, sval);
+                        q[c] = qv;
+                        a0 += (double)sc_ * (double)qv;
+                    }
+                }
+                put3(j, a0, 0.0, 0.0);
+            }
+            if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+            reduce(1, [&](int, SceneLocal& P, double sq, double, double) -> bool {
+                if (P.inner_done) return false;
+                P.alpha = sq != 0.0 ? P.rho / sq : 0.0;
+                float sq32 = (float)sq;
+                P.alpha32 = sq32 != 0.0f ? P.rho32 / sq32 : 0.0f;
+                return true;
+            });
+            for (int j = 0;; ++j) {
+                int s;
+                long long t0, t1;
+                if (!chunk_of(j, s, t0, t1)) break;
+                double a0 = 0.0, a1 = 0.0;
+                if (!L[s].inner_done) {
+                    const T al = (T)L[s].alpha32;
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = cell_at(j, t, t0);
+                        T sv = s_cur[c];
+                        T xv = x[c] + al * sv;
+                        T rv = r[c] + (-al) * q[c];
+                        x[c] = xv;
+                        r[c] = rv;
+                        a0 += (double)rv * (double)rv;
+                        T zv = precond(c, rv);
+                        z[c] = zv;
+                        a1 += (double)zv * (double)rv;
+                    }
+                }
+                put3(j, a0, a1, 0.0);
+            }
+            if (!count_barrier(A.bar, S.dev_error, ++epoch, tmo)) return;
+            int act = reduce(2, [&](int s, SceneLocal& P, double rr, double rho2, double) -> bool {
+                if (P.inner_done) return false;
+                const int n = S.scenes[s].n;
+                P.iters += 1;
+                P.rr = rr;
+                const int cap = A.max_iters > 0 ? A.max_iters : n * n * n;
+                bool conv = (float)rr <= (float)P.target;
+                if (conv || P.iters >= cap) {
+                    P.inner_done = 1;
+                    P.done = 1;
+                    P.converged = conv;
+                    return false;
+                }
+                P.beta = P.rho != 0.0 ? rho2 / P.rho : 0.0;
+                P.rho = rho2;
+                float r32 = (float)rho2;
+                P.beta32 = P.rho32 != 0.0f ? r32 / P.rho32 : 0.0f;
+                P.rho32 = r32;
+                return true;
+            });
+            if (act == 0) break;
+        }
+        break;
+    }
+
+    // ---- results: final per-scene state and totals (block 0), fp32 pressure ---------------
+    if (blockIdx.x == 0) {
+        for (int s = threadIdx.x; s < k; s += blockDim.x) {
+            const SceneLocal& P = L[s];
+            PcgScene o = load_sc(A.sc + s);
+            o.bb = P.bb;
+            o.rr = P.rr;
+            o.rho = P.rho;
+            o.alpha = P.alpha;
+            o.beta = P.beta;
+            o.rr_out = P.rr_out;
+            o.target = P.target;
+            o.iters = P.iters;
+            o.outer = P.outer;
+            o.done = P.done;
+            o.inner_done = P.inner_done;
+            o.converged = P.converged;
+            A.sc[s] = o;
+            PcgTotals& Tt = A.totals[s];
+            Tt.solves += 1;
+            Tt.iterations += P.iters;
+            Tt.outer += MODE == kMixed ? P.outer : 1;
+            Tt.cell_iterations += (double)P.nf * (double)P.iters;
+            Tt.cell_outer += (double)P.nf * (double)(MODE == kMixed ? P.outer : 1);
+            Tt.not_converged += P.converged ? 0 : 1;
+        }
+    }
+    if (MODE != kRef32) {
+        // P64 of this block's cells was written by this block above (no barrier needed)
+        for (int j = 0;; ++j) {
+            int s;
+            long long t0, t1;
+            if (!chunk_of(j, s, t0, t1)) break;
+            for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                long long c = cell_at(j, t, t0);
+                S.P[c] = (float)S.P64[c];
+            }
+        }
+    }
+}
+
 template <int MODE>
 static cudaError_t coop_launch(const PcgArgs& A, int nblocks, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
@@ -942,7 +1706,37 @@ static cudaError_t coop_launch(const PcgArgs& A, int nblocks, cudaStream_t st) {
     return e;
 }
 
+template <int MODE>
+static cudaError_t coop_launch_fast(const PcgArgs& A, int nblocks, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nblocks);
+    cfg.blockDim = dim3(kPcgThreads);
+    cfg.dynamicSmemBytes = fast_dyn_smem(MODE);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg_fast<MODE>, A);
+    count_launch();
+    return e;
+}
+
+// With the reference preconditioner and few enough scenes the fast kernel solves and the
+// general kernel returns at once; with an ordered preconditioner it is the other way round
+// (the choice is made on the device, from the preparation's FLUID-cell scan).
 cudaError_t launch_pcg_solve(const PcgArgs& A, int nblocks, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    if (A.fast) {
+        switch (A.mode) {
+            case kRef32: e = coop_launch_fast<kRef32>(A, nblocks, st); break;
+            case kFp64: e = coop_launch_fast<kFp64>(A, nblocks, st); break;
+            default: e = coop_launch_fast<kMixed>(A, nblocks, st); break;
+        }
+        if (e != cudaSuccess) return e;
+        if (A.precond != ARIEL_PRECOND_MIC0 && !A.may_be_ordered) return e;
+    }
     switch (A.mode) {
         case kRef32: return coop_launch<kRef32>(A, nblocks, st);
         case kFp64: return coop_launch<kFp64>(A, nblocks, st);
@@ -950,20 +1744,31 @@ cudaError_t launch_pcg_solve(const PcgArgs& A, int nblocks, cudaStream_t st) {
     }
 }
 
-int pcg_max_blocks(int device, int mode) {
+int pcg_max_blocks(int device, int mode, int per_sm_cap) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaError_t e;
-    if (mode == kRef32)
+    int per_fast = 0;
+    const int dyn = (int)fast_dyn_smem(mode);
+    if (mode == kRef32) {
+        cudaFuncSetAttribute(k_pcg_fast<kRef32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kRef32>, kPcgThreads, 0);
-    else if (mode == kFp64)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kRef32>, kPcgThreads, dyn);
+    } else if (mode == kFp64) {
+        cudaFuncSetAttribute(k_pcg_fast<kFp64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kFp64>, kPcgThreads, 0);
-    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kFp64>, kPcgThreads, dyn);
+    } else {
+        cudaFuncSetAttribute(k_pcg_fast<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kMixed>, kPcgThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kMixed>, kPcgThreads, dyn);
+    }
+    if (per_fast < per) per = per_fast;  // one grid size serves both kernels
     if (e != cudaSuccess || per < 1) per = 1;
-    // Two blocks per SM cover the FLUID chunks of the bench sizes; more blocks only lengthen
-    // every grid barrier.
-    return sms * (per < 2 ? per : 2);
+    // The default of two blocks per SM covers the FLUID chunks of the bench sizes; more blocks
+    // add arrivals to every grid barrier.
+    int cap = per_sm_cap > 0 ? per_sm_cap : 2;
+    return sms * (per < cap ? per : cap);
 }
 
 cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long timeout_ns, cudaStream_t st) {

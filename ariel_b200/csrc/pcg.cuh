@@ -52,6 +52,8 @@ struct Barrier {
 struct PcgArgs {
     DevState S;
     int mode;
+    int fast;            // k_pcg_fast handles launches without an ordered preconditioner
+    int may_be_ordered;  // the general kernel must also be launched (see launch_pcg_solve)
     int precond;
     int stop_rule;
     int max_iters;     // <=0: n^3 per scene
@@ -77,9 +79,14 @@ struct PcgArgs {
     void* s1;
     void* q;
     void* ordq;      // forward-sweep scratch of the ordered preconditioner
+    void* u;         // single-reduction PCG: preconditioned residual
+    void* p;         // single-reduction PCG: search direction
+    void* va0;       // fast single-reduction PCG: packed (r, w, s, pc), two parities
+    void* va1;
+    void* vb;        // fast single-reduction PCG: packed (u, p, x, -)
     double* r64;     // MIXED outer residual
     float* d32;      // MIXED inner correction
-    double* partial; // 3 * max chunks
+    double* partial; // 3 * max chunks (three dot products per reduction)
     long long max_chunks;
     PcgScene* sc;
     PcgTotals* totals;
@@ -92,7 +99,7 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
 // The cooperative persistent PCG kernel.
 cudaError_t launch_pcg_solve(const PcgArgs& A, int nblocks, cudaStream_t st);
 // Blocks of the persistent kernel that fit on the device at once.
-int pcg_max_blocks(int device, int mode);
+int pcg_max_blocks(int device, int mode, int per_sm_cap);
 // Bounded-wait self test (one arrival missing).
 cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long timeout_ns, cudaStream_t st);
 

@@ -155,7 +155,7 @@ typedef struct AsimParams {
     double barrier_timeout_ms;/* bound of every device-side spin wait */
     int32_t fail_on_not_converged; /* return ARIEL_ERR_NOT_CONVERGED from step when a solve
                                       stops at max_iters above tolerance */
-    int32_t reserved;
+    int32_t pcg_blocks_per_sm;  /* blocks per SM of the persistent solve kernel; 0 = default (2) */
 } AsimParams;
 
 typedef struct AsimStats {
