@@ -46,7 +46,12 @@ struct SceneDev {
     long long f_begin;
     unsigned long long rng_seed;
     int resample_every;  // resample on frames divisible by this (1: every step, flip.cpp:121)
-    int pad;
+    // When a kernel radius squared (in float) is a power of two, r2 / (h*h) equals
+    // r2 * (1 / (h*h)) exactly, so the division can be replaced by a multiplication.
+    int dens_pow2;       // dens_h * dens_h is a power of two
+    float dens_inv_hh;
+    int re_pow2;         // resample_re^2 is a power of two
+    float re_inv_hh;
 };
 
 // ------------------------------------------------------------------------------------------
@@ -68,6 +73,15 @@ __device__ __forceinline__ float sqrlength(float ax, float ay, float az, float b
     return a * a + b * b + c * c;
 }
 __device__ __forceinline__ float smooth_k(float r2, float h) { return gmax(1.0f - r2 / (h * h), 0.0f); }
+// smooth_k with the division replaced by an exact power-of-two reciprocal when pow2 is set.
+__device__ __forceinline__ float smooth_fast(float r2, float h, int pow2, float inv_hh) {
+    return pow2 ? gmax(1.0f - r2 * inv_hh, 0.0f) : smooth_k(r2, h);
+}
+// Squared distance from x to the interval [lo, hi] along one axis.
+__device__ __forceinline__ float axis_gap2(float x, float lo, float hi) {
+    float d = x < lo ? lo - x : (x > hi ? x - hi : 0.0f);
+    return d * d;
+}
 __device__ __forceinline__ float sharpen_k(float r2, float h) {
     return gmax(h * h / gmax(r2, 1.0e-5f) - 1.0f, 0.0f);
 }

@@ -313,6 +313,14 @@ SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
                                   d.solid[i].center[2] * D.maxd, d.solid[i].radius * D.maxd);
     D.rng_seed = p.rng_seed;
     D.resample_every = p.resample_every;
+    auto pow2 = [](float v, float* inv) {
+        int e = 0;
+        float m = std::frexp(v, &e);
+        *inv = 1.0f / v;
+        return (m == 0.5f && std::isfinite(*inv) && *inv * v == 1.0f) ? 1 : 0;
+    };
+    D.dens_pow2 = pow2(D.dens_h * D.dens_h, &D.dens_inv_hh);
+    D.re_pow2 = pow2(D.resample_re * D.resample_re, &D.re_inv_hh);
     return D;
 }
 
@@ -379,6 +387,7 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     ARIEL_TRY(dalloc(s, &S.sid, np));
     ARIEL_TRY(dalloc(s, &S.spos4, np));
     ARIEL_TRY(dalloc(s, &S.svel4, np));
+    ARIEL_TRY(dalloc(s, &S.gpos4, np));
     ARIEL_TRY(dalloc(s, &S.dens, np));
     ARIEL_TRY(dalloc(s, &s->d_dens_id, np));
     ARIEL_TRY(dalloc(s, &s->d_stage, 6 * (size_t)np));

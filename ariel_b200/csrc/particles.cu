@@ -189,11 +189,27 @@ __global__ void k_sort_cells(DevState S) {
 }
 
 __global__ void k_sort_permute(DevState S) {
+    SCENE_PREFIX(S.p_pref);
     long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S.np) return;
     uint32_t g = S.sid[s];
-    S.spos4[s] = S.pos4[g];
-    S.svel4[s] = S.vel4[g];
+    float4 p = S.pos4[g];
+    float4 v = S.vel4[g];
+    S.spos4[s] = p;
+    S.svel4[s] = v;
+    // SplatParticlesToMACGrid's clamped grid position (particlegridoperations.inl:172-174);
+    // non-FLUID particles are placed out of every face's reach (they are skipped, :170)
+    const float maxd = S.scenes[find_scene(pref_s, S.k, s)].maxd;
+    float4 gp;
+    if (type_of(v) == ARIEL_FLUID) {
+        gp.x = gmax(0.0f, gmin(maxd, maxd * p.x));
+        gp.y = gmax(0.0f, gmin(maxd, maxd * p.y));
+        gp.z = gmax(0.0f, gmin(maxd, maxd * p.z));
+        gp.w = p.w;
+    } else {
+        gp = make_float4(1.0e30f, 1.0e30f, 1.0e30f, 0.0f);
+    }
+    S.gpos4[s] = gp;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -223,7 +239,7 @@ __global__ void k_density(DevState S) {
             for (uint32_t t = a; t < b; ++t) {
                 float4 q = S.spos4[t];
                 float sqd = sqrlength(q.x, q.y, q.z, p.x, p.y, p.z);
-                float weight = q.w * smooth_k(sqd, hk);
+                float weight = q.w * smooth_fast(sqd, hk, D.dens_pow2, D.dens_inv_hh);
                 weightsum = weightsum + weight;
             }
         }
@@ -307,23 +323,30 @@ __global__ void k_p2g(DevState S) {
     zlo = max(zlo, 0); zhi = min(zhi, n - 1);
     const float RE = 1.4f;
     const float RE2 = RE * RE;
-    const float maxd = D.maxd;
+    // Cells whose nearest point is farther than the Sharpen radius (with a 10% margin over any
+    // rounding) hold only particles whose weight is exactly 0; skipping them leaves the
+    // contributing particles in the reference's order.
+    const float LIM = 1.1f * RE2;
     float sumw = 0.0f, sumu = 0.0f;
     if (zlo <= zhi) {
         for (int sx = xlo; sx <= xhi; ++sx) {
+            const float gx = axis_gap2(fx, (float)sx, (float)(sx + 1));
+            if (gx > LIM) continue;
             for (int sy = ylo; sy <= yhi; ++sy) {
+                const float gxy = gx + axis_gap2(fy, (float)sy, (float)(sy + 1));
+                if (gxy > LIM) continue;
+                int z0 = zlo, z1 = zhi;
+                while (z0 <= z1 && gxy + axis_gap2(fz, (float)z0, (float)(z0 + 1)) > LIM) ++z0;
+                while (z1 >= z0 && gxy + axis_gap2(fz, (float)z1, (float)(z1 + 1)) > LIM) --z1;
+                if (z0 > z1) continue;
                 long long cb = D.c_begin + ((long long)sx * n + sy) * n;
-                uint32_t a = S.start[cb + zlo], b = S.start[cb + zhi + 1];
+                uint32_t a = S.start[cb + z0], b = S.start[cb + z1 + 1];
                 for (uint32_t t = a; t < b; ++t) {
-                    float4 v = S.svel4[t];
-                    if (type_of(v) != ARIEL_FLUID) continue;
-                    float4 q = S.spos4[t];
-                    float px = gmax(0.0f, gmin(maxd, maxd * q.x));
-                    float py = gmax(0.0f, gmin(maxd, maxd * q.y));
-                    float pz = gmax(0.0f, gmin(maxd, maxd * q.z));
-                    float r2 = sqrlength(px, py, pz, fx, fy, fz);
-                    // Sharpen is exactly 0 for r2 >= RE^2, so such particles add nothing.
+                    float4 q = S.gpos4[t];
+                    float r2 = sqrlength(q.x, q.y, q.z, fx, fy, fz);
+                    // Sharpen is exactly 0 for r2 >= RE^2 (and non-FLUID records are far away)
                     if (!(r2 < RE2)) continue;
+                    float4 v = S.svel4[t];
                     float w = q.w * sharpen_k(r2, RE);
                     float uc = axis == 0 ? v.x : (axis == 1 ? v.y : v.z);
                     sumu += w * uc;
@@ -435,6 +458,14 @@ __global__ void k_g2p_advect(DevState S) {
 // one thread per slot of the resampler's own Sort.  rand() becomes Philox keyed by
 // (rng seed, frame, particle id, draw ordinal).
 // ------------------------------------------------------------------------------------------
+// Gap from x to cell c's box along one axis (unit coordinates); the boxes of the first and last
+// cell extend to infinity because Sort clamps outside particles into them.
+__device__ __forceinline__ float cell_gap2(float x, int c, int n, float ch) {
+    float lo = c == 0 ? -INFINITY : c * ch;
+    float hi = c == n - 1 ? INFINITY : (c + 1) * ch;
+    return axis_gap2(x, lo, hi);
+}
+
 __device__ __forceinline__ void nb_range(float x, int n, int& lo, int& hi) {
     // GetCellNeighbors with a fractional index and radius 1 (particlegrid.cpp:32-35)
     lo = (int)(x - 1.0f);
@@ -443,109 +474,161 @@ __device__ __forceinline__ void nb_range(float x, int n, int& lo, int& hi) {
     if (hi > n - 1) hi = n - 1;
 }
 
-__global__ void k_resample(DevState S) {
+constexpr int kResList = 16;
+
+// Cells along one axis that can hold a particle within sqrt(lim) of x (unit coordinates):
+// the particle's own cell c, plus c-1 / c+1 when their box is that close; clipped to the
+// reference's neighbour range [lo, hi].  Visiting the selected cells in lexicographic order
+// visits the contributing particles in ascending slot order, which is the reference's order.
+__device__ __forceinline__ void axis_cells(float x, int c, int n, float ch, float lim, int& lo, int& hi) {
+    int a = c, b = c;
+    if (c - 1 >= lo && cell_gap2(x, c - 1, n, ch) <= lim) a = c - 1;
+    if (c + 1 <= hi && cell_gap2(x, c + 1, n, ch) <= lim) b = c + 1;
+    if (c < lo || c > hi) {  // own cell outside the range (clamped positions): keep the range
+        a = lo;
+        b = hi;
+    }
+    lo = a;
+    hi = b;
+}
+
+// The resampler runs as two kernels over the slots of its own Sort: springs (the target
+// position t), then the velocity at t and the acceptance.  In both, each thread walks the 27
+// neighbour cells of the reference (threads of one cell share them, so a warp stays
+// together) testing only distance, records the few candidates in ascending slot order --
+// the reference's summation order -- and then evaluates them with the reference's exact
+// arithmetic.  Neighbours that fail the test contribute exactly nothing.
+__global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
     SCENE_PREFIX(S.p_pref);
-    long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ uint32_t lst[kResList][kBlock];
+    const int me = threadIdx.x;
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S.np) return;
-    float4 p4 = S.spos4[s];
-    float4 v4 = S.svel4[s];
-    if (type_of(v4) != ARIEL_FLUID) return;
+    const float4 p4 = S.spos4[s];
+    if (type_of(S.svel4[s]) != ARIEL_FLUID) return;
     const SceneDev& D = S.scenes[find_scene(pref_s, S.k, s)];
     if (D.resample_every <= 0 || D.frame % D.resample_every != 0) return;
     const int n = D.n;
     const float maxd = D.maxd;
     const float dt = D.dt;
     const float re = D.resample_re;
-    const float springforce = 50.0f;
-    const float re2 = re * re;
-    const uint32_t g = S.sid[s];
-    const uint32_t gid = (uint32_t)(g - D.p_begin);
-    const uint32_t k0 = (uint32_t)D.rng_seed, k1 = (uint32_t)(D.rng_seed >> 32);
+    const float near2 = 2.0f * re * re;  // beyond this the spring term is exactly zero
+    const uint32_t gid = (uint32_t)(S.sid[s] - D.p_begin);
+    uint32_t draws = 0;
     float3 spring = make_float3(0, 0, 0);
-    {
-        float x = gmax(0.0f, gmin(maxd, maxd * p4.x));
-        float y = gmax(0.0f, gmin(maxd, maxd * p4.y));
-        float z = gmax(0.0f, gmin(maxd, maxd * p4.z));
-        int xl, xh, yl, yh, zl, zh;
-        nb_range(x, n, xl, xh);
-        nb_range(y, n, yl, yh);
-        nb_range(z, n, zl, zh);
-        uint32_t draws = 0;
-        if (zl <= zh) {
-            for (int sx = xl; sx <= xh; ++sx)
-                for (int sy = yl; sy <= yh; ++sy) {
-                    long long cb = D.c_begin + ((long long)sx * n + sy) * n;
-                    uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
-                    for (uint32_t t = a; t < b; ++t) {
-                        if (t == (uint32_t)s) continue;
-                        float4 q = S.spos4[t];
-                        float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
-                        float dd = gdot3(d, d);
-                        // Beyond twice re^2 the Smooth weight is exactly 0 and the jitter branch
-                        // (dist <= 0.1 re) cannot trigger, so the neighbour adds exactly nothing.
-                        if (!(dd < 2.0f * re2)) continue;
-                        float dist = sqrtf(dd);
-                        if (!(dist * dist < re2) && dist > 0.1f * re) continue;  // w == 0 exactly
-                        float w = springforce * q.w * smooth_k(dist * dist, re);
-                        if (dist > 0.1f * re) {
-                            spring.x += w * (p4.x - q.x) / dist * re;
-                            spring.y += w * (p4.y - q.y) / dist * re;
-                            spring.z += w * (p4.z - q.z) / dist * re;
-                        } else if (type_of(S.svel4[t]) == ARIEL_FLUID) {
-                            uint4 rv = philox4x32_10(make_uint4(gid, (uint32_t)D.frame, draws++, kTagResample), k0, k1);
-                            spring.x += 0.01f * re / dt * (float)(rv.x % 101u) / 100.0f;
-                            spring.y += 0.01f * re / dt * (float)(rv.y % 101u) / 100.0f;
-                            spring.z += 0.01f * re / dt * (float)(rv.z % 101u) / 100.0f;
-                        } else {
-                            // SOLID neighbour: its normal m_n is zero for scene-generated solids
-                            spring.x += 0.05f * re / dt * 0.0f;
-                            spring.y += 0.05f * re / dt * 0.0f;
-                            spring.z += 0.05f * re / dt * 0.0f;
-                        }
+    // particleresampler.inl:58-78 for one neighbour slot t
+    auto eval = [&](uint32_t t) {
+        const float springforce = 50.0f;
+        float4 q = S.spos4[t];
+        float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
+        float dist = sqrtf(gdot3(d, d));
+        float w = springforce * q.w * smooth_fast(dist * dist, re, D.re_pow2, D.re_inv_hh);
+        if (dist > 0.1f * re) {
+            spring.x += w * (p4.x - q.x) / dist * re;
+            spring.y += w * (p4.y - q.y) / dist * re;
+            spring.z += w * (p4.z - q.z) / dist * re;
+        } else if (type_of(S.svel4[t]) == ARIEL_FLUID) {
+            uint4 rv = philox4x32_10(make_uint4(gid, (uint32_t)D.frame, draws++, kTagResample),
+                                     (uint32_t)D.rng_seed, (uint32_t)(D.rng_seed >> 32));
+            spring.x += 0.01f * re / dt * (float)(rv.x % 101u) / 100.0f;
+            spring.y += 0.01f * re / dt * (float)(rv.y % 101u) / 100.0f;
+            spring.z += 0.01f * re / dt * (float)(rv.z % 101u) / 100.0f;
+        } else {
+            // SOLID neighbour: its normal m_n is zero for scene-generated solids
+            spring.x += 0.05f * re / dt * 0.0f;
+            spring.y += 0.05f * re / dt * 0.0f;
+            spring.z += 0.05f * re / dt * 0.0f;
+        }
+    };
+    int xl, xh, yl, yh, zl, zh;
+    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.x)), n, xl, xh);
+    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.y)), n, yl, yh);
+    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.z)), n, zl, zh);
+    int nl = 0;
+    if (zl <= zh) {
+        for (int sx = xl; sx <= xh; ++sx)
+            for (int sy = yl; sy <= yh; ++sy) {
+                const long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                const uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                for (uint32_t t = a; t < b; ++t) {
+                    const float4 q = S.spos4[t];
+                    const float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
+                    if (!(gdot3(d, d) < near2) || t == (uint32_t)s) continue;
+                    lst[nl][me] = t;
+                    if (++nl == kResList) {
+                        for (int i = 0; i < nl; ++i) eval(lst[i][me]);
+                        nl = 0;
                     }
                 }
-        }
+            }
     }
-    float3 t;
-    t.x = p4.x + dt * spring.x;
-    t.y = p4.y + dt * spring.y;
-    t.z = p4.z + dt * spring.z;
-    // Resample (particleresampler.inl:120-148)
+    for (int i = 0; i < nl; ++i) eval(lst[i][me]);
+    float4 t4;
+    t4.x = p4.x + dt * spring.x;
+    t4.y = p4.y + dt * spring.y;
+    t4.z = p4.z + dt * spring.z;
+    t4.w = 0.0f;
+    S.gpos4[s] = t4;  // the P2G records are rebuilt by the next Sort
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
+    SCENE_PREFIX(S.p_pref);
+    __shared__ uint32_t lst[kResList][kBlock];
+    const int me = threadIdx.x;
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S.np) return;
+    const float4 v4 = S.svel4[s];
+    if (type_of(v4) != ARIEL_FLUID) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, s)];
+    if (D.resample_every <= 0 || D.frame % D.resample_every != 0) return;
+    const int n = D.n;
+    const float maxd = D.maxd;
+    const float re = D.resample_re;
+    const float re2 = re * re;
+    const float4 t4 = S.gpos4[s];
+    const float3 t = make_float3(t4.x, t4.y, t4.z);
     float wsum = 0.0f;
     float3 ru = make_float3(0, 0, 0);
-    {
-        float x = gmax(0.0f, gmin(maxd - 1, maxd * t.x));
-        float y = gmax(0.0f, gmin(maxd - 1, maxd * t.y));
-        float z = gmax(0.0f, gmin(maxd - 1, maxd * t.z));
-        int xl, xh, yl, yh, zl, zh;
-        nb_range(x, n, xl, xh);
-        nb_range(y, n, yl, yh);
-        nb_range(z, n, zl, zh);
-        if (zl <= zh) {
-            for (int sx = xl; sx <= xh; ++sx)
-                for (int sy = yl; sy <= yh; ++sy) {
-                    long long cb = D.c_begin + ((long long)sx * n + sy) * n;
-                    uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
-                    for (uint32_t q = a; q < b; ++q) {
-                        float4 np = S.spos4[q];
-                        float dist2 = sqrlength(t.x, t.y, t.z, np.x, np.y, np.z);
-                        // Sharpen is exactly 0 for dist2 >= re^2
-                        if (!(dist2 < re2)) continue;
-                        float4 nv = S.svel4[q];
-                        if (type_of(nv) != ARIEL_FLUID) continue;
-                        float w = np.w * sharpen_k(dist2, re);
-                        ru.x = ru.x + w * nv.x;
-                        ru.y = ru.y + w * nv.y;
-                        ru.z = ru.z + w * nv.z;
-                        wsum += w;
+    // Resample (particleresampler.inl:133-141) for one neighbour slot
+    auto eval = [&](uint32_t q) {
+        float4 nv = S.svel4[q];
+        if (type_of(nv) != ARIEL_FLUID) return;
+        float4 np = S.spos4[q];
+        float dist2 = sqrlength(t.x, t.y, t.z, np.x, np.y, np.z);
+        float w = np.w * sharpen_k(dist2, re);
+        ru.x = ru.x + w * nv.x;
+        ru.y = ru.y + w * nv.y;
+        ru.z = ru.z + w * nv.z;
+        wsum += w;
+    };
+    int xl, xh, yl, yh, zl, zh;
+    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.x)), n, xl, xh);
+    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.y)), n, yl, yh);
+    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.z)), n, zl, zh);
+    int nl = 0;
+    if (zl <= zh) {
+        for (int sx = xl; sx <= xh; ++sx)
+            for (int sy = yl; sy <= yh; ++sy) {
+                const long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+                const uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                for (uint32_t q = a; q < b; ++q) {
+                    const float4 np = S.spos4[q];
+                    // Sharpen is exactly 0 for dist2 >= re^2
+                    if (!(sqrlength(t.x, t.y, t.z, np.x, np.y, np.z) < re2)) continue;
+                    lst[nl][me] = q;
+                    if (++nl == kResList) {
+                        for (int i = 0; i < nl; ++i) eval(lst[i][me]);
+                        nl = 0;
                     }
                 }
-        }
+            }
     }
+    for (int i = 0; i < nl; ++i) eval(lst[i][me]);
     if (wsum != 0.0f)
         ru = f3div(ru, wsum);
     else
         ru = make_float3(v4.x, v4.y, v4.z);
+    const float4 p4 = S.spos4[s];
     float3 p = make_float3(p4.x, p4.y, p4.z);
     float3 u = make_float3(v4.x, v4.y, v4.z);
     if (!(D.n_spheres > 0 && inside_solid(D, f3mul(t, maxd)))) {
@@ -554,6 +637,7 @@ __global__ void k_resample(DevState S) {
     }
     if (D.n_spheres > 0)
         solid_constraints(D, p, u, make_float3(p4.x, p4.y, p4.z), make_float3(v4.x, v4.y, v4.z));
+    const uint32_t g = S.sid[s];
     S.pos4[g] = make_float4(p.x, p.y, p.z, p4.w);
     S.vel4[g] = make_float4(u.x, u.y, u.z, v4.w);
 }
@@ -686,8 +770,9 @@ cudaError_t launch_resample(const DevState& S, void* scan_tmp, cudaStream_t st) 
     cudaError_t e = sort_core(S, scan_tmp, st);
     if (e != cudaSuccess) return e;
     if (S.np == 0) return cudaSuccess;
-    k_resample<<<grid_for(S.np), kBlock, 0, st>>>(S);
-    count_launch();
+    k_resample_spring<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    k_resample_velocity<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    count_launch(2);
     return cudaGetLastError();
 }
 

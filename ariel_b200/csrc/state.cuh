@@ -28,6 +28,8 @@ struct DevState {
     uint32_t* sid;    // slot -> packed particle id (ascending inside a cell)
     float4* spos4;    // slot copies
     float4* svel4;
+    float4* gpos4;    // slot -> P2G record: clamped grid position and mass (FLUID), far away
+                      // for other particles so that they fall outside every face's radius
     float* dens;      // slot -> density
     // static solid particles binned by cell (positions never change)
     uint32_t* solid_start;  // nc+1
