@@ -14,11 +14,12 @@ ARIEL_ERR_CUDA = 5
 ARIEL_ERR_STATE = 6
 ARIEL_ERR_NO_DEVICE = 7
 ARIEL_ERR_NAN = 8
+ARIEL_ERR_PENDING = 9
 
 STATUS_NAMES = {
     0: "ARIEL_OK", 1: "ARIEL_ERR_INVALID_ARG", 2: "ARIEL_ERR_OOM", 3: "ARIEL_ERR_NOT_CONVERGED",
     4: "ARIEL_ERR_DEVICE_TIMEOUT", 5: "ARIEL_ERR_CUDA", 6: "ARIEL_ERR_STATE",
-    7: "ARIEL_ERR_NO_DEVICE", 8: "ARIEL_ERR_NAN",
+    7: "ARIEL_ERR_NO_DEVICE", 8: "ARIEL_ERR_NAN", 9: "ARIEL_ERR_PENDING",
 }
 
 AIR, FLUID, SOLID = 0, 1, 2          # src/grid/macgrid.inl:13
@@ -88,6 +89,39 @@ class AsimSolverTotals(C.Structure):
         ("solves", C.c_int64), ("iterations", C.c_int64), ("outer", C.c_int64),
         ("cell_iterations", C.c_double), ("cell_outer", C.c_double),
         ("not_converged", C.c_int64), ("reserved", C.c_int64),
+    ]
+
+
+REQ_QUEUED, REQ_READY, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
+
+
+class AsimServerConfig(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_int64), ("max_live", C.c_int32), ("prepare_threads", C.c_int32),
+        ("keep_results", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+class AsimRequestInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_int32), ("status", C.c_int32), ("nsteps", C.c_int32), ("steps_done", C.c_int32),
+        ("n_particles", C.c_int64), ("state_bytes", C.c_int64),
+        ("submit_ms", C.c_double), ("admit_ms", C.c_double), ("done_ms", C.c_double),
+        ("stats", AsimStats),
+    ]
+
+
+class AsimServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("admitted", C.c_int64), ("finished", C.c_int64),
+        ("failed", C.c_int64), ("live", C.c_int64), ("waiting", C.c_int64),
+        ("batch_steps", C.c_int64), ("particle_steps", C.c_int64), ("timed_steps", C.c_int64),
+        ("wall_ms", C.c_double), ("busy_ms", C.c_double),
+        ("step_ms_p50", C.c_double), ("step_ms_p99", C.c_double), ("step_ms_max", C.c_double),
+        ("latency_ms_p50", C.c_double), ("latency_ms_p99", C.c_double),
+        ("relayouts", C.c_int64), ("relayout_ms", C.c_double),
+        ("hbm_budget_bytes", C.c_int64), ("hbm_in_use_bytes", C.c_int64), ("hbm_peak_bytes", C.c_int64),
+        ("max_live_seen", C.c_int32), ("last_error", C.c_int32),
     ]
 
 

@@ -47,6 +47,18 @@ SIGNATURES = {
     "ariel_kernel_launches": ([], C.c_int64),
     "ariel_last_error": ([], C.c_char_p),
     "ariel_sort_by_cell_noalloc": ([_vp, C.c_int64, C.c_int32, _vp, _vp, _vp, _vp], C.c_int),
+    "ariel_server_config_default": ([C.POINTER(A.AsimServerConfig)], None),
+    "ariel_server_create": ([C.POINTER(A.AsimParams), C.POINTER(A.AsimServerConfig), C.POINTER(_vp)], C.c_int),
+    "ariel_server_submit": ([_vp, C.POINTER(A.AsimSceneDesc), C.c_int32, C.POINTER(C.c_int64)], C.c_int),
+    "ariel_server_poll": ([_vp, C.c_int64, C.POINTER(A.AsimRequestInfo)], C.c_int),
+    "ariel_server_wait": ([_vp, C.c_int64, C.c_double], C.c_int),
+    "ariel_server_drain": ([_vp, C.c_double], C.c_int),
+    "ariel_server_fetch": ([_vp, C.c_int64, _vp, _vp], C.c_int),
+    "ariel_server_release": ([_vp, C.c_int64], C.c_int),
+    "ariel_server_stats": ([_vp, C.POINTER(A.AsimServerStats)], C.c_int),
+    "ariel_server_shutdown": ([_vp], C.c_int),
+    "ariel_state_bytes": ([C.POINTER(A.AsimSceneDesc), C.c_int32, C.POINTER(A.AsimParams),
+                           C.POINTER(C.c_int64)], C.c_int),
 }
 
 

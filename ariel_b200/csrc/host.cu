@@ -8,147 +8,37 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
-#include "pcg.cuh"
+#include "sim.cuh"
 
 using namespace ariel;
 
 namespace {
 
-struct DeviceBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
 thread_local char g_last_error[256] = "";
 
-#define ARIEL_CUDA(call)                                                        \
-    do {                                                                        \
-        cudaError_t e_ = (call);                                                \
-        if (e_ != cudaSuccess) return map_cuda_error(e_, #call);                \
+#define ARIEL_CUDA(call)                                                                    \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) return ::ariel::hostimpl::map_cuda_error(e_, #call);         \
     } while (0)
 
-ariel_status map_cuda_error(cudaError_t e, const char* what = "") {
-    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
-    if (e == cudaErrorMemoryAllocation) return ARIEL_ERR_OOM;
-    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ARIEL_ERR_NO_DEVICE;
-    return ARIEL_ERR_CUDA;
-}
-
-// Every copy goes through the handle's stream (non-blocking, so the legacy default stream would
-// not be ordered with the kernels) and is waited for before returning.
-cudaError_t copy_sync(cudaStream_t st, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
-    if (bytes == 0) return cudaSuccess;
-    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    return e;
-}
-
-// Host copy of the per-scene particle arrays (id order) used while (re)building packed state.
-struct HostParticles {
-    std::vector<float4> pos4;  // x y z mass
-    std::vector<float4> vel4;  // u v w type-bits
-};
-
-inline float4 pack_vel(float u, float v, float w, int type) {
-    float4 r;
-    r.x = u;
-    r.y = v;
-    r.z = w;
-    int t = type;
-    std::memcpy(&r.w, &t, 4);
-    return r;
-}
-inline int type_bits(const float4& v) {
-    int t;
-    std::memcpy(&t, &v.w, 4);
-    return t;
-}
+#define ARIEL_TRY(x)                          \
+    do {                                      \
+        ariel_status st_ = (x);               \
+        if (st_ != ARIEL_OK) return st_;      \
+    } while (0)
 
 inline float hmin(float x, float y) { return (y < x) ? y : x; }  // glm::min
 inline float hmax(float x, float y) { return (x < y) ? y : x; }  // glm::max
-
-// Scene::GenerateParticles (src/scene/scene.cpp:257-360) for box liquids and analytic sphere
-// solids, placed in lexicographic (i,j,k) lattice order: liquid particles first, then solids
-// (scene.cpp:349-354).  Liquid particles may be jittered inside their lattice sub-cell by
-// Philox4x32-10 keyed by (seed, particle index, box).
-void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
-    const int n = d.dim;
-    const float maxdim = (float)n;
-    const float thickness = 1.0f / maxdim;
-    const float density = d.density;
-    const float w = density * thickness;
-    const uint32_t k0 = (uint32_t)d.seed, k1 = (uint32_t)(d.seed >> 32);
-    auto inside_solid = [&](float x, float y, float z) {
-        for (int s = 0; s < d.n_solid; ++s) {
-            float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
-                  cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
-            float dx = x - cx, dy = y - cy, dz = z - cz;
-            float dd = (dx * dx + dy * dy) + dz * dz;
-            if (dd < r * r) return true;
-        }
-        return false;
-    };
-    out.pos4.clear();
-    out.vel4.clear();
-    for (int l = 0; l < d.n_liquid; ++l) {
-        const AsimBox& bx = d.liquid[l];
-        float lminx = hmax(std::floor(bx.lo[0] * maxdim), 0.0f) / density;
-        float lminy = hmax(std::floor(bx.lo[1] * maxdim), 0.0f) / density;
-        float lminz = hmax(std::floor(bx.lo[2] * maxdim), 0.0f) / density;
-        float lmaxx = hmin(std::ceil(bx.hi[0] * maxdim), maxdim + 1.0f) / density;
-        float lmaxy = hmin(std::ceil(bx.hi[1] * maxdim), maxdim + 1.0f) / density;
-        float lmaxz = hmin(std::ceil(bx.hi[2] * maxdim), maxdim + 1.0f) / density;
-        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
-            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
-                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
-                    float cx = (i * w) + (w / 2.0f), cy = (j * w) + (w / 2.0f), cz = (k * w) + (w / 2.0f);
-                    float wx = cx * maxdim, wy = cy * maxdim, wz = cz * maxdim;
-                    bool inside = wx > bx.lo[0] * maxdim && wx < bx.hi[0] * maxdim && wy > bx.lo[1] * maxdim &&
-                                  wy < bx.hi[1] * maxdim && wz > bx.lo[2] * maxdim && wz < bx.hi[2] * maxdim;
-                    if (!inside || inside_solid(wx, wy, wz)) continue;
-                    float px = cx, py = cy, pz = cz;
-                    if (d.jitter > 0.0f) {
-                        uint32_t id = (uint32_t)out.pos4.size();
-                        uint4 rv = philox4x32_10(make_uint4(id, (uint32_t)l, 0u, kTagSeed), k0, k1);
-                        float ux = (float)(rv.x >> 8) * (1.0f / 16777216.0f);
-                        float uy = (float)(rv.y >> 8) * (1.0f / 16777216.0f);
-                        float uz = (float)(rv.z >> 8) * (1.0f / 16777216.0f);
-                        px = (i * w) + (ux * w);
-                        py = (j * w) + (uy * w);
-                        pz = (k * w) + (uz * w);
-                    }
-                    out.pos4.push_back(make_float4(px, py, pz, 1.0f));
-                    out.vel4.push_back(pack_vel(bx.vel[0], bx.vel[1], bx.vel[2], ARIEL_FLUID));
-                }
-    }
-    for (int s = 0; s < d.n_solid; ++s) {
-        float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
-              cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
-        float lminx = hmax(std::floor(cx - r), 0.0f) / density;
-        float lminy = hmax(std::floor(cy - r), 0.0f) / density;
-        float lminz = hmax(std::floor(cz - r), 0.0f) / density;
-        float lmaxx = hmin(std::ceil(cx + r), maxdim + 1.0f) / density;
-        float lmaxy = hmin(std::ceil(cy + r), maxdim + 1.0f) / density;
-        float lmaxz = hmin(std::ceil(cz + r), maxdim + 1.0f) / density;
-        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
-            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
-                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
-                    float px = (i * w) + (w / 2.0f), py = (j * w) + (w / 2.0f), pz = (k * w) + (w / 2.0f);
-                    float wx = px * maxdim - cx, wy = py * maxdim - cy, wz = pz * maxdim - cz;
-                    float dd = (wx * wx + wy * wy) + wz * wz;
-                    if (!(dd < r * r)) continue;
-                    out.pos4.push_back(make_float4(px, py, pz, 10.0f));
-                    out.vel4.push_back(pack_vel(0.0f, 0.0f, 0.0f, ARIEL_SOLID));
-                }
-    }
-}
 
 // FlipSim::Init's density normaliser (flip.cpp:42-70): density of a 10x10x10 lattice of
 // unit-mass FLUID particles at spacing density/maxd, max over the lattice.  One block per
@@ -206,85 +96,261 @@ __global__ void k_max_density(SceneDev* scenes, int k) {
     }
 }
 
-}  // namespace
+// dst[i] = (src ? src[i] : 0) + add: places a scene's solid bins at their packed offset.
+__global__ void k_u32_offset(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src, long long n, uint32_t add) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = (src ? src[i] : 0u) + add;
+}
 
-constexpr int kEvSolveKernel = ARIEL_STAGE_COUNT + 1;
-constexpr int kEvCount = ARIEL_STAGE_COUNT + 2;
-
-struct ariel_sim {
-    int device = 0;
-    int k = 0;
-    std::vector<AsimSceneDesc> descs;
-    AsimParams prm{};
-    std::vector<SceneDev> sh;  // host mirror of the scene table
-    std::vector<long long> ppref, cpref, fpref;
-    long long np = 0, nc = 0, nf = 0;
-    bool any_solid = false;
-    bool inited = false;
-    cudaStream_t stream = nullptr;
-    std::vector<DeviceBuf> bufs;
-    // device pointers
-    SceneDev* d_scenes = nullptr;
-    long long *d_ppref = nullptr, *d_cpref = nullptr, *d_fpref = nullptr;
-    DevState S{};
-    PcgArgs PA{};
-    void* scan_tmp = nullptr;
-    uint32_t *flpred = nullptr, *flscan = nullptr;
-    float* d_dens_id = nullptr;
-    int pcg_blocks = 0;
-    int mode = kRef32;
-    // graphs of one whole step: [0] plain, [1],[2] with the two stage-event sets
-    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-    bool graph_tried[3] = {false, false, false};
-    long long graph_kernels[3] = {0, 0, 0};
-    // timing: two event sets (stage boundaries + solve-kernel start), used alternately so that
-    // one step's events are read while the next step runs
-    cudaEvent_t ev[2][kEvCount] = {};
-    bool ev_pending[2] = {false, false};
-    int ev_slot = 0;
-    double acc_stage[ARIEL_STAGE_COUNT] = {};
-    double acc_solve_kernel = 0;
-    std::vector<double> step_hist;
-    cudaEvent_t tb = nullptr, te = nullptr;
-    double stage_ms[ARIEL_STAGE_COUNT] = {};
-    double step_ms = 0;
-    float* d_stage = nullptr;  // xyz staging for host-buffer particle I/O
-    int last_status = ARIEL_OK;
-    std::vector<int64_t> frames;
-};
-
-namespace {
+cudaError_t launch_u32_offset(uint32_t* dst, const uint32_t* src, long long n, uint32_t add, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_u32_offset<<<grid_for(n), kBlock, 0, st>>>(dst, src, n, add);
+    count_launch();
+    return cudaGetLastError();
+}
 
 template <class T>
-ariel_status dalloc(ariel_sim* s, T** p, size_t count) {
+ariel_status dalloc(ariel_sim* s, T** p, size_t count, bool keep = false) {
     *p = nullptr;
     if (count == 0) count = 1;
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+    const size_t bytes = count * sizeof(T);
+    cudaError_t e = s->pool ? cudaMallocFromPoolAsync(&q, bytes, s->pool, s->stream) : cudaMalloc(&q, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return ARIEL_ERR_OOM;
     }
-    s->bufs.push_back(DeviceBuf{q, count * sizeof(T)});
+    s->bufs.push_back(DeviceBuf{q, bytes, keep, s->pool != nullptr});
     *p = (T*)q;
     return ARIEL_OK;
 }
 
-void free_all(ariel_sim* s) {
+void destroy_graphs(ariel_sim* s) {
     for (int i = 0; i < 3; ++i) {
         if (s->graph[i]) cudaGraphExecDestroy(s->graph[i]);
         s->graph[i] = nullptr;
         s->graph_tried[i] = false;
     }
-    for (auto& b : s->bufs) cudaFree(b.p);
-    s->bufs.clear();
 }
 
-#define ARIEL_TRY(x)                          \
-    do {                                      \
-        ariel_status st_ = (x);               \
-        if (st_ != ARIEL_OK) return st_;      \
-    } while (0)
+void free_bufs(ariel_sim* s, bool scratch_only) {
+    destroy_graphs(s);
+    std::vector<DeviceBuf> left;
+    for (auto& b : s->bufs) {
+        if (scratch_only && b.keep) {
+            left.push_back(b);
+            continue;
+        }
+        if (b.pooled)
+            cudaFreeAsync(b.p, s->stream);
+        else
+            cudaFree(b.p);
+    }
+    s->bufs.swap(left);
+}
+
+void free_all(ariel_sim* s) { free_bufs(s, false); }
+
+// Buffer sizes of one packed layout.
+struct Layout {
+    long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0;
+    bool any_solid = false;
+    int mode = kRef32;
+};
+
+int mode_of(const AsimParams& p) {
+    return p.precision == ARIEL_PREC_FP64 ? kFp64 : (p.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
+}
+
+constexpr long long kChunkCells = 1024;  // the fast solve kernel's fixed chunk size
+
+// The allocation list of build_state, in bytes (each buffer rounded to 256 bytes as the
+// allocators place them).  Kept next to build_state; a GPU test holds the two equal.
+long long layout_bytes(const Layout& L) {
+    long long total = 0;
+    auto add = [&](long long count, long long esize) {
+        long long b = std::max(1ll, count) * esize;
+        total += (b + 255) / 256 * 256;
+    };
+    const long long k = L.k, np = L.np, nc = L.nc, nf = L.nf;
+    add(k, sizeof(SceneDev));
+    for (int i = 0; i < 3; ++i) add(k + 1, 8);
+    add(np, 16);
+    add(np, 16);
+    if (L.any_solid) {
+        add(np, 16);
+        add(np, 16);
+    }
+    add(np, 4);  // key
+    add(np, 4);  // off
+    add(nc, 4);  // count
+    add(nc + 1, 4);  // start
+    add(np, 4);   // sid
+    add(np, 16);  // spos4
+    add(np, 16);  // svel4
+    add(np, 16);  // gpos4
+    add(np, 4);   // dens
+    add(np, 4);   // dens by id
+    add(6 * np, 4);  // host I/O staging
+    add(nc + 1, 4);  // solid_start
+    add(nc, 1);      // flags
+    add(nc, 4);      // L
+    add(nc, 4);      // D
+    add(nc, 4);      // P
+    add(nc, 8);      // P64
+    add(nf, 4);      // u
+    add(nf, 4);      // pu
+    add(1, 4);       // dev_error
+    add((long long)scan_tmp_bytes(nc), 1);
+    add(nc, 4);      // FLUID list
+    add(k + 1, 8);
+    add(k + 1, 8);
+    add(nc, 4);      // flpred
+    add(nc + 1, 4);  // flscan
+    add(nc, 1);      // mask
+    add(nc, 8);      // diag
+    add(nc, 8);      // pc64
+    add(nc, 4);      // pc32
+    const long long vb = L.mode == kFp64 ? 8 : 4;
+    for (int i = 0; i < 8; ++i) add(nc, vb);
+    for (int i = 0; i < 3; ++i) add(4 * nc, vb);
+    if (L.mode == kMixed) {
+        add(nc, 8);
+        add(nc, 4);
+    }
+    add(3 * std::max(1ll, L.maxch), 8);
+    add(k, sizeof(PcgScene));
+    add(k, sizeof(PcgTotals));
+    add(1, sizeof(PcgCtl));
+    add(1, sizeof(Barrier));
+    add(L.ns, 16);  // solid_pos
+    return total;
+}
+
+}  // namespace
+
+namespace ariel {
+namespace hostimpl {
+
+ariel_status map_cuda_error(cudaError_t e, const char* what) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return ARIEL_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return ARIEL_ERR_NO_DEVICE;
+    return ARIEL_ERR_CUDA;
+}
+
+// Every copy goes through the handle's stream (non-blocking, so the legacy default stream would
+// not be ordered with the kernels) and is waited for before returning.
+cudaError_t copy_sync(cudaStream_t st, void* dst, const void* src, size_t bytes, cudaMemcpyKind kind) {
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
+// Scene::GenerateParticles (src/scene/scene.cpp:257-360) for box liquids and analytic sphere
+// solids, placed in lexicographic (i,j,k) lattice order: liquid particles first, then solids
+// (scene.cpp:349-354).  Liquid particles may be jittered inside their lattice sub-cell by
+// Philox4x32-10 keyed by (seed, particle index, box).
+void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
+    const int n = d.dim;
+    const float maxdim = (float)n;
+    const float thickness = 1.0f / maxdim;
+    const float density = d.density;
+    const float w = density * thickness;
+    const uint32_t k0 = (uint32_t)d.seed, k1 = (uint32_t)(d.seed >> 32);
+    auto inside_solid = [&](float x, float y, float z) {
+        for (int s = 0; s < d.n_solid; ++s) {
+            float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
+                  cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
+            float dx = x - cx, dy = y - cy, dz = z - cz;
+            float dd = (dx * dx + dy * dy) + dz * dz;
+            if (dd < r * r) return true;
+        }
+        return false;
+    };
+    out = HostParticles{};
+    for (int l = 0; l < d.n_liquid; ++l) {
+        const AsimBox& bx = d.liquid[l];
+        float lminx = hmax(std::floor(bx.lo[0] * maxdim), 0.0f) / density;
+        float lminy = hmax(std::floor(bx.lo[1] * maxdim), 0.0f) / density;
+        float lminz = hmax(std::floor(bx.lo[2] * maxdim), 0.0f) / density;
+        float lmaxx = hmin(std::ceil(bx.hi[0] * maxdim), maxdim + 1.0f) / density;
+        float lmaxy = hmin(std::ceil(bx.hi[1] * maxdim), maxdim + 1.0f) / density;
+        float lmaxz = hmin(std::ceil(bx.hi[2] * maxdim), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    float cx = (i * w) + (w / 2.0f), cy = (j * w) + (w / 2.0f), cz = (k * w) + (w / 2.0f);
+                    float wx = cx * maxdim, wy = cy * maxdim, wz = cz * maxdim;
+                    bool inside = wx > bx.lo[0] * maxdim && wx < bx.hi[0] * maxdim && wy > bx.lo[1] * maxdim &&
+                                  wy < bx.hi[1] * maxdim && wz > bx.lo[2] * maxdim && wz < bx.hi[2] * maxdim;
+                    if (!inside || inside_solid(wx, wy, wz)) continue;
+                    float px = cx, py = cy, pz = cz;
+                    if (d.jitter > 0.0f) {
+                        uint32_t id = (uint32_t)out.pos4.size();
+                        uint4 rv = philox4x32_10(make_uint4(id, (uint32_t)l, 0u, kTagSeed), k0, k1);
+                        float ux = (float)(rv.x >> 8) * (1.0f / 16777216.0f);
+                        float uy = (float)(rv.y >> 8) * (1.0f / 16777216.0f);
+                        float uz = (float)(rv.z >> 8) * (1.0f / 16777216.0f);
+                        px = (i * w) + (ux * w);
+                        py = (j * w) + (uy * w);
+                        pz = (k * w) + (uz * w);
+                    }
+                    out.pos4.push_back(make_float4(px, py, pz, 1.0f));
+                    out.vel4.push_back(pack_vel(bx.vel[0], bx.vel[1], bx.vel[2], ARIEL_FLUID));
+                }
+    }
+    for (int s = 0; s < d.n_solid; ++s) {
+        float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
+              cz = d.solid[s].center[2] * maxdim, r = d.solid[s].radius * maxdim;
+        float lminx = hmax(std::floor(cx - r), 0.0f) / density;
+        float lminy = hmax(std::floor(cy - r), 0.0f) / density;
+        float lminz = hmax(std::floor(cz - r), 0.0f) / density;
+        float lmaxx = hmin(std::ceil(cx + r), maxdim + 1.0f) / density;
+        float lmaxy = hmin(std::ceil(cy + r), maxdim + 1.0f) / density;
+        float lmaxz = hmin(std::ceil(cz + r), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    float px = (i * w) + (w / 2.0f), py = (j * w) + (w / 2.0f), pz = (k * w) + (w / 2.0f);
+                    float wx = px * maxdim - cx, wy = py * maxdim - cy, wz = pz * maxdim - cz;
+                    float dd = (wx * wx + wy * wy) + wz * wz;
+                    if (!(dd < r * r)) continue;
+                    out.pos4.push_back(make_float4(px, py, pz, 10.0f));
+                    out.vel4.push_back(pack_vel(0.0f, 0.0f, 0.0f, ARIEL_SOLID));
+                }
+    }
+    bin_solids(d, out);
+}
+
+// Static SOLID particles binned by cell, id order inside a cell: their positions never change
+// (only FLUID particles are moved by any stage of the step), so the bins are built once.
+void bin_solids(const AsimSceneDesc& d, HostParticles& hp) {
+    hp.solid_pos.clear();
+    hp.solid_start.clear();
+    hp.binned = true;
+    const long long n = d.dim;
+    const float maxd = (float)n;
+    std::vector<std::pair<long long, float4>> sol;
+    for (size_t p = 0; p < hp.pos4.size(); ++p) {
+        if (type_bits(hp.vel4[p]) != ARIEL_SOLID) continue;
+        const float4& q = hp.pos4[p];
+        auto cc = [&](float x) { return (long long)(int)hmax(0.0f, hmin((float)(int)maxd - 1.0f, (float)(int)maxd * x)); };
+        sol.push_back({(cc(q.x) * n + cc(q.y)) * n + cc(q.z), q});
+    }
+    if (sol.empty()) return;
+    std::stable_sort(sol.begin(), sol.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const long long ncell = n * n * n;
+    hp.solid_start.assign(ncell + 1, 0);
+    hp.solid_pos.resize(sol.size());
+    for (size_t i = 0; i < sol.size(); ++i) {
+        hp.solid_start[sol[i].first + 1]++;
+        hp.solid_pos[i] = sol[i].second;
+    }
+    for (long long c = 0; c < ncell; ++c) hp.solid_start[c + 1] += hp.solid_start[c];
+}
 
 SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
     SceneDev D{};
@@ -334,30 +400,64 @@ ariel_status validate(const AsimSceneDesc& d) {
     return ARIEL_OK;
 }
 
-// (Re)allocate every buffer for the current scene list and particle counts, upload the
-// particles given per scene, and bin the static SOLID particles.
-ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
+long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector<long long>& particles,
+                      const std::vector<long long>& solids, const AsimParams& prm) {
+    Layout L;
+    L.k = (long long)descs.size();
+    L.mode = mode_of(prm);
+    for (size_t i = 0; i < descs.size(); ++i) {
+        const long long n = descs[i].dim;
+        L.np += particles[i];
+        L.nc += n * n * n;
+        L.nf += 3 * n * n * (n + 1);
+        L.ns += solids[i];
+        L.maxch += (n * n * n + kChunkCells - 1) / kChunkCells;
+        if (descs[i].n_solid > 0) L.any_solid = true;
+    }
+    return layout_bytes(L);
+}
+
+void free_scratch(ariel_sim* s) { free_bufs(s, true); }
+
+ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ariel_sim* src,
+                         const std::vector<int>* src_idx) {
     free_all(s);
     const int k = s->k;
+    auto from_src = [&](int i) { return src && src_idx && (*src_idx)[i] >= 0; };
+    for (int i = 0; i < k; ++i)
+        if (!from_src(i) && !hp[i].binned) bin_solids(s->descs[i], hp[i]);
     s->ppref.assign(k + 1, 0);
     s->cpref.assign(k + 1, 0);
     s->fpref.assign(k + 1, 0);
+    s->spref.assign(k + 1, 0);
     s->any_solid = false;
+    long long maxch = 0;
     for (int i = 0; i < k; ++i) {
         long long n = s->descs[i].dim;
-        s->ppref[i + 1] = s->ppref[i] + (long long)hp[i].pos4.size();
+        long long cnt, scnt;
+        if (from_src(i)) {
+            const int j = (*src_idx)[i];
+            cnt = src->ppref[j + 1] - src->ppref[j];
+            scnt = src->spref[j + 1] - src->spref[j];
+        } else {
+            cnt = (long long)hp[i].pos4.size();
+            scnt = (long long)hp[i].solid_pos.size();
+        }
+        s->ppref[i + 1] = s->ppref[i] + cnt;
         s->cpref[i + 1] = s->cpref[i] + n * n * n;
         s->fpref[i + 1] = s->fpref[i] + 3 * n * n * (n + 1);
+        s->spref[i + 1] = s->spref[i] + scnt;
         s->sh[i].p_begin = s->ppref[i];
         s->sh[i].p_end = s->ppref[i + 1];
         s->sh[i].c_begin = s->cpref[i];
         s->sh[i].f_begin = s->fpref[i];
         if (s->descs[i].n_solid > 0) s->any_solid = true;
+        maxch += (n * n * n + kChunkCells - 1) / kChunkCells;
     }
     s->np = s->ppref[k];
     s->nc = s->cpref[k];
     s->nf = s->fpref[k];
-    if (s->np >= (1ll << 31) || s->nc >= (1ll << 31)) return ARIEL_ERR_INVALID_ARG;
+    if (s->np >= (1ll << 31) || s->nc >= (1ll << 31) || s->spref[k] >= (1ll << 32)) return ARIEL_ERR_INVALID_ARG;
     const long long np = s->np, nc = s->nc, nf = s->nf;
     DevState& S = s->S;
     S = DevState{};
@@ -366,7 +466,8 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     S.np = np;
     S.nc = nc;
     S.nf = nf;
-    ARIEL_TRY(dalloc(s, &s->d_scenes, k));
+    // The order and sizes of these allocations are mirrored by layout_bytes.
+    ARIEL_TRY(dalloc(s, &s->d_scenes, k, true));
     ARIEL_TRY(dalloc(s, &s->d_ppref, k + 1));
     ARIEL_TRY(dalloc(s, &s->d_cpref, k + 1));
     ARIEL_TRY(dalloc(s, &s->d_fpref, k + 1));
@@ -374,8 +475,8 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     S.p_pref = s->d_ppref;
     S.c_pref = s->d_cpref;
     S.f_pref = s->d_fpref;
-    ARIEL_TRY(dalloc(s, &S.pos4, np));
-    ARIEL_TRY(dalloc(s, &S.vel4, np));
+    ARIEL_TRY(dalloc(s, &S.pos4, np, true));
+    ARIEL_TRY(dalloc(s, &S.vel4, np, true));
     if (s->any_solid) {
         ARIEL_TRY(dalloc(s, &S.pt4, np));
         ARIEL_TRY(dalloc(s, &S.ut4, np));
@@ -391,12 +492,12 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     ARIEL_TRY(dalloc(s, &S.dens, np));
     ARIEL_TRY(dalloc(s, &s->d_dens_id, np));
     ARIEL_TRY(dalloc(s, &s->d_stage, 6 * (size_t)np));
-    ARIEL_TRY(dalloc(s, &S.solid_start, nc + 1));
+    ARIEL_TRY(dalloc(s, &S.solid_start, nc + 1, true));
     ARIEL_TRY(dalloc(s, &S.flags, nc));
     ARIEL_TRY(dalloc(s, &S.L, nc));
     ARIEL_TRY(dalloc(s, &S.D, nc));
-    ARIEL_TRY(dalloc(s, &S.P, nc));
-    ARIEL_TRY(dalloc(s, &S.P64, nc));
+    ARIEL_TRY(dalloc(s, &S.P, nc, true));
+    ARIEL_TRY(dalloc(s, &S.P64, nc, true));
     ARIEL_TRY(dalloc(s, &S.u, nf));
     ARIEL_TRY(dalloc(s, &S.pu, nf));
     ARIEL_TRY(dalloc(s, &S.dev_error, 1));
@@ -407,13 +508,13 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
     // pressure solve
     PcgArgs& A = s->PA;
     A = PcgArgs{};
-    s->mode = s->prm.precision == ARIEL_PREC_FP64 ? kFp64 : (s->prm.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
+    s->mode = mode_of(s->prm);
     A.mode = s->mode;
     A.precond = s->prm.precond;
     A.stop_rule = s->prm.stop_rule;
     A.max_iters = s->prm.max_iters;
     A.max_outer = s->prm.max_outer > 0 ? s->prm.max_outer : 8;
-    A.chunk = 1024;  // the fast solve kernel's fixed chunk size
+    A.chunk = (int)kChunkCells;
     A.fast = (k <= 128 && A.precond == ARIEL_PRECOND_REF) ? 1 : 0;
     // the reference preconditioner needs the ordered kernel only in the rare PRef == 1 case,
     // which only the device knows; keep launching it (it returns at once when not needed)
@@ -458,65 +559,79 @@ ariel_status build_state(ariel_sim* s, const std::vector<HostParticles>& hp) {
         ARIEL_TRY(dalloc(s, &A.r64, nc));
         ARIEL_TRY(dalloc(s, &A.d32, nc));
     }
-    long long maxch = 0;
-    for (int i = 0; i < k; ++i) {
-        long long n = s->descs[i].dim;
-        maxch += (n * n * n + A.chunk - 1) / A.chunk;
-    }
     A.max_chunks = std::max(1ll, maxch);
     ARIEL_TRY(dalloc(s, &A.partial, 3 * A.max_chunks));
-    ARIEL_TRY(dalloc(s, &A.sc, k));
-    ARIEL_TRY(dalloc(s, &A.totals, k));
-    ARIEL_CUDA(cudaMemsetAsync(A.totals, 0, sizeof(PcgTotals) * k, s->stream));
+    ARIEL_TRY(dalloc(s, &A.sc, k, true));
+    ARIEL_TRY(dalloc(s, &A.totals, k, true));
     ARIEL_TRY(dalloc(s, &A.ctl, 1));
     ARIEL_TRY(dalloc(s, &A.bar, 1));
+    ARIEL_TRY(dalloc(s, &S.solid_pos, s->spref[k], true));
     A.S = S;
     s->pcg_blocks = pcg_max_blocks(s->device, s->mode, s->prm.pcg_blocks_per_sm);
-    // uploads
-    ARIEL_CUDA(cudaMemcpyAsync(s->d_scenes, s->sh.data(), sizeof(SceneDev) * k, cudaMemcpyHostToDevice, s->stream));
-    ARIEL_CUDA(cudaMemcpyAsync(s->d_ppref, s->ppref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
-    ARIEL_CUDA(cudaMemcpyAsync(s->d_cpref, s->cpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
-    ARIEL_CUDA(cudaMemcpyAsync(s->d_fpref, s->fpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, s->stream));
+    cudaStream_t st = s->stream;
+    // scene table and prefixes
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_scenes, s->sh.data(), sizeof(SceneDev) * k, cudaMemcpyHostToDevice, st));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_ppref, s->ppref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, st));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_cpref, s->cpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, st));
+    ARIEL_CUDA(cudaMemcpyAsync(s->d_fpref, s->fpref.data(), sizeof(long long) * (k + 1), cudaMemcpyHostToDevice, st));
+    ARIEL_CUDA(cudaMemsetAsync(S.P, 0, sizeof(float) * nc, st));
+    ARIEL_CUDA(cudaMemsetAsync(S.P64, 0, sizeof(double) * nc, st));
+    ARIEL_CUDA(cudaMemsetAsync(S.dev_error, 0, sizeof(int), st));
+    ARIEL_CUDA(cudaMemsetAsync(S.u, 0, sizeof(float) * nf, st));
+    ARIEL_CUDA(cudaMemsetAsync(S.pu, 0, sizeof(float) * nf, st));
+    ARIEL_CUDA(cudaMemsetAsync(S.flags, 0, nc, st));
+    ARIEL_CUDA(cudaMemsetAsync(A.sc, 0, sizeof(PcgScene) * k, st));
+    ARIEL_CUDA(cudaMemsetAsync(A.totals, 0, sizeof(PcgTotals) * k, st));
+    // per-scene persistent state
+    uint32_t* stage_u32 = nullptr;
     for (int i = 0; i < k; ++i) {
-        size_t cnt = hp[i].pos4.size();
-        if (cnt == 0) continue;
-        ARIEL_CUDA(copy_sync(s->stream, S.pos4 + s->ppref[i], hp[i].pos4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
-        ARIEL_CUDA(copy_sync(s->stream, S.vel4 + s->ppref[i], hp[i].vel4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
-    }
-    ARIEL_CUDA(cudaMemsetAsync(S.P, 0, sizeof(float) * nc, s->stream));
-    ARIEL_CUDA(cudaMemsetAsync(S.P64, 0, sizeof(double) * nc, s->stream));
-    ARIEL_CUDA(cudaMemsetAsync(S.dev_error, 0, sizeof(int), s->stream));
-    ARIEL_CUDA(cudaMemsetAsync(S.u, 0, sizeof(float) * nf, s->stream));
-    ARIEL_CUDA(cudaMemsetAsync(S.pu, 0, sizeof(float) * nf, s->stream));
-    ARIEL_CUDA(cudaMemsetAsync(S.flags, 0, nc, s->stream));
-    // static SOLID particles binned by cell, id order inside a cell (positions never change:
-    // only FLUID particles are moved by any stage of the step)
-    std::vector<uint32_t> sstart(nc + 1, 0);
-    std::vector<std::pair<long long, float4>> sol;
-    for (int i = 0; i < k; ++i) {
-        const long long n = s->descs[i].dim;
-        const float maxd = (float)n;
-        for (size_t p = 0; p < hp[i].pos4.size(); ++p) {
-            if (type_bits(hp[i].vel4[p]) != ARIEL_SOLID) continue;
-            const float4& q = hp[i].pos4[p];
-            auto cc = [&](float x) { return (long long)(int)hmax(0.0f, hmin((float)(int)maxd - 1.0f, (float)(int)maxd * x)); };
-            long long c = s->cpref[i] + (cc(q.x) * n + cc(q.y)) * n + cc(q.z);
-            sol.push_back({c, q});
+        const long long pb = s->ppref[i], cnt = s->ppref[i + 1] - pb;
+        const long long cb = s->cpref[i], ncell = s->cpref[i + 1] - cb;
+        const long long sb = s->spref[i], scnt = s->spref[i + 1] - sb;
+        if (from_src(i)) {
+            // a scene carried over from another layout: device copies, solid offsets shifted
+            const int j = (*src_idx)[i];
+            const long long pb0 = src->ppref[j], cb0 = src->cpref[j], sb0 = src->spref[j];
+            const DevState& T = src->S;
+            if (cnt > 0) {
+                ARIEL_CUDA(cudaMemcpyAsync(S.pos4 + pb, T.pos4 + pb0, cnt * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+                ARIEL_CUDA(cudaMemcpyAsync(S.vel4 + pb, T.vel4 + pb0, cnt * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+            }
+            ARIEL_CUDA(cudaMemcpyAsync(S.P + cb, T.P + cb0, ncell * sizeof(float), cudaMemcpyDeviceToDevice, st));
+            ARIEL_CUDA(cudaMemcpyAsync(S.P64 + cb, T.P64 + cb0, ncell * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if (scnt > 0)
+                ARIEL_CUDA(cudaMemcpyAsync(S.solid_pos + sb, T.solid_pos + sb0, scnt * sizeof(float4),
+                                           cudaMemcpyDeviceToDevice, st));
+            ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, T.solid_start + cb0, ncell, 0u, st));
+            if (sb != sb0) {
+                // shift in place: offsets of this scene move from sb0 to sb
+                ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, S.solid_start + cb, ncell, (uint32_t)(sb - sb0), st));
+            }
+            ARIEL_CUDA(cudaMemcpyAsync(A.sc + i, src->PA.sc + j, sizeof(PcgScene), cudaMemcpyDeviceToDevice, st));
+            ARIEL_CUDA(cudaMemcpyAsync(A.totals + i, src->PA.totals + j, sizeof(PcgTotals), cudaMemcpyDeviceToDevice, st));
+            continue;
+        }
+        if (cnt > 0) {
+            ARIEL_CUDA(copy_sync(st, S.pos4 + pb, hp[i].pos4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
+            ARIEL_CUDA(copy_sync(st, S.vel4 + pb, hp[i].vel4.data(), cnt * sizeof(float4), cudaMemcpyHostToDevice));
+        }
+        if (scnt > 0) {
+            ARIEL_CUDA(copy_sync(st, S.solid_pos + sb, hp[i].solid_pos.data(), scnt * sizeof(float4), cudaMemcpyHostToDevice));
+            if (!stage_u32) {
+                // the scene-local offsets pass through the I/O staging area when it is large
+                // enough, else through a temporary buffer
+                ARIEL_CUDA(cudaMallocAsync(&stage_u32, sizeof(uint32_t) * (size_t)(s->nc + 1), st));
+            }
+            ARIEL_CUDA(copy_sync(st, stage_u32, hp[i].solid_start.data(), ncell * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, stage_u32, ncell, (uint32_t)sb, st));
+        } else {
+            ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, nullptr, ncell, (uint32_t)sb, st));
         }
     }
-    std::stable_sort(sol.begin(), sol.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    std::vector<float4> spos(sol.size());
-    for (size_t i = 0; i < sol.size(); ++i) {
-        sstart[sol[i].first + 1]++;
-        spos[i] = sol[i].second;
-    }
-    for (long long c = 0; c < nc; ++c) sstart[c + 1] += sstart[c];
-    ARIEL_TRY(dalloc(s, &S.solid_pos, spos.size()));
-    if (!spos.empty())
-        ARIEL_CUDA(copy_sync(s->stream, S.solid_pos, spos.data(), spos.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    ARIEL_CUDA(copy_sync(s->stream, S.solid_start, sstart.data(), sstart.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ARIEL_CUDA(launch_u32_offset(S.solid_start + nc, nullptr, 1, (uint32_t)s->spref[k], st));
+    if (stage_u32) ARIEL_CUDA(cudaFreeAsync(stage_u32, st));
     s->PA.S = S;
-    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    ARIEL_CUDA(cudaStreamSynchronize(st));
     return ARIEL_OK;
 }
 
@@ -533,6 +648,84 @@ ariel_status check_device_error(ariel_sim* s) {
     }
     return ARIEL_OK;
 }
+
+ariel_status compute_max_density(ariel_sim* s) {
+    k_max_density<<<s->k, 1024, 0, s->stream>>>(s->d_scenes, s->k);
+    count_launch();
+    ARIEL_CUDA(cudaGetLastError());
+    std::vector<SceneDev> dev(s->k);
+    ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < s->k; ++i) s->sh[i].max_density = dev[i].max_density;
+    return ARIEL_OK;
+}
+
+ariel_status refresh_scene_table(ariel_sim* s) {
+    std::vector<SceneDev> dev(s->k);
+    ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < s->k; ++i) {
+        s->sh[i].frame = dev[i].frame;
+        s->sh[i].max_density = dev[i].max_density;
+    }
+    return ARIEL_OK;
+}
+
+ariel_status sort_and_classify_init(ariel_sim* s) {
+    cudaError_t e = launch_sort(s->S, s->scan_tmp, s->stream);
+    if (e == cudaSuccess) e = launch_fill_dens(s->S, 10.0f, s->stream);  // AddLiquidParticle: m_density = 10
+    if (e == cudaSuccess) e = launch_classify(s->S, 1, s->stream);
+    if (e != cudaSuccess) return map_cuda_error(e);
+    return ARIEL_OK;
+}
+
+ariel_status new_sim(const AsimSceneDesc* descs, int k, const AsimParams& prm, cudaStream_t stream,
+                     cudaMemPool_t pool, ariel_sim** out) {
+    *out = nullptr;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    ariel_sim* s = new (std::nothrow) ariel_sim();
+    if (!s) return ARIEL_ERR_OOM;
+    s->device = dev;
+    s->k = k;
+    s->descs.assign(descs, descs + k);
+    s->prm = prm;
+    s->frames.assign(k, 0);
+    for (int i = 0; i < k; ++i) s->sh.push_back(make_scene(descs[i], prm));
+    s->pool = pool;
+    if (stream) {
+        s->stream = stream;
+        s->own_stream = false;
+    } else if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return ARIEL_ERR_CUDA;
+    }
+    for (auto& set : s->ev)
+        for (auto& e : set) cudaEventCreate(&e);
+    cudaEventCreate(&s->tb);
+    cudaEventCreate(&s->te);
+    *out = s;
+    return ARIEL_OK;
+}
+
+void delete_sim(ariel_sim* s) {
+    if (!s) return;
+    cudaStreamSynchronize(s->stream);
+    free_all(s);
+    cudaStreamSynchronize(s->stream);
+    for (auto& set : s->ev)
+        for (auto& e : set) cudaEventDestroy(e);
+    cudaEventDestroy(s->tb);
+    cudaEventDestroy(s->te);
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+}  // namespace hostimpl
+}  // namespace ariel
+
+using namespace ariel::hostimpl;
+
+namespace {
 
 ariel_status enqueue_stage(ariel_sim* s, int g, cudaEvent_t* evs = nullptr) {
     const DevState& S = s->S;
@@ -620,14 +813,6 @@ void try_build_graph(ariel_sim* s, int which) {
     count_launch(-(int)kernels);  // capture does not launch; replays are counted instead
 }
 
-ariel_status sort_and_classify_init(ariel_sim* s) {
-    cudaError_t e = launch_sort(s->S, s->scan_tmp, s->stream);
-    if (e == cudaSuccess) e = launch_fill_dens(s->S, 10.0f, s->stream);  // AddLiquidParticle: m_density = 10
-    if (e == cudaSuccess) e = launch_classify(s->S, 1, s->stream);
-    if (e != cudaSuccess) return map_cuda_error(e);
-    return ARIEL_OK;
-}
-
 ariel_status download_particles(ariel_sim* s, std::vector<HostParticles>& hp) {
     hp.assign(s->k, HostParticles{});
     for (int i = 0; i < s->k; ++i) {
@@ -641,13 +826,14 @@ ariel_status download_particles(ariel_sim* s, std::vector<HostParticles>& hp) {
     return ARIEL_OK;
 }
 
-ariel_status create_common(const AsimSceneDesc* descs, int32_t k, const AsimParams* params, ariel_sim** out) {
-    if (!descs || !params || !out || k < 1 || k > kMaxScenes) return ARIEL_ERR_INVALID_ARG;
-    *out = nullptr;
-    for (int i = 0; i < k; ++i) ARIEL_TRY(validate(descs[i]));
+ariel_status check_params(const AsimParams* params) {
     if (params->precision < 0 || params->precision > 2 || params->precond < 0 || params->precond > 1 ||
         params->stop_rule < 0 || params->stop_rule > 1)
         return ARIEL_ERR_INVALID_ARG;
+    return ARIEL_OK;
+}
+
+ariel_status check_device() {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
         cudaGetLastError();
@@ -658,28 +844,21 @@ ariel_status create_common(const AsimSceneDesc* descs, int32_t k, const AsimPara
     int major = 0;
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     if (major != 10) return ARIEL_ERR_NO_DEVICE;  // built for sm_100a only
-    ariel_sim* s = new (std::nothrow) ariel_sim();
-    if (!s) return ARIEL_ERR_OOM;
-    s->device = dev;
-    s->k = k;
-    s->descs.assign(descs, descs + k);
-    s->prm = *params;
-    s->frames.assign(k, 0);
-    for (int i = 0; i < k; ++i) s->sh.push_back(make_scene(descs[i], *params));
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete s;
-        return ARIEL_ERR_CUDA;
-    }
-    for (auto& set : s->ev)
-        for (auto& e : set) cudaEventCreate(&e);
-    cudaEventCreate(&s->tb);
-    cudaEventCreate(&s->te);
+    return ARIEL_OK;
+}
+
+ariel_status create_common(const AsimSceneDesc* descs, int32_t k, const AsimParams* params, ariel_sim** out) {
+    if (!descs || !params || !out || k < 1 || k > kMaxScenes) return ARIEL_ERR_INVALID_ARG;
+    *out = nullptr;
+    for (int i = 0; i < k; ++i) ARIEL_TRY(validate(descs[i]));
+    ARIEL_TRY(check_params(params));
+    ARIEL_TRY(check_device());
+    ariel_sim* s = nullptr;
+    ARIEL_TRY(new_sim(descs, k, *params, nullptr, nullptr, &s));
     std::vector<HostParticles> empty(k);
     ariel_status st = build_state(s, empty);
     if (st != ARIEL_OK) {
-        free_all(s);
-        cudaStreamDestroy(s->stream);
-        delete s;
+        delete_sim(s);
         return st;
     }
     *out = s;
@@ -687,6 +866,50 @@ ariel_status create_common(const AsimSceneDesc* descs, int32_t k, const AsimPara
 }
 
 }  // namespace
+
+namespace ariel {
+namespace hostimpl {
+
+ariel_status step_async(ariel_sim* s) {
+    if (s->prm.timing) {
+        const int slot = s->ev_slot;
+        s->ev_slot ^= 1;
+        if (s->ev_pending[slot]) ARIEL_TRY(collect_step_events(s, slot));
+        if (s->prm.use_graph && !s->graph_tried[1 + slot]) try_build_graph(s, 1 + slot);
+        if (s->graph[1 + slot]) {
+            cudaError_t e = cudaGraphLaunch(s->graph[1 + slot], s->stream);
+            if (e != cudaSuccess) return map_cuda_error(e);
+            count_launch((int)s->graph_kernels[1 + slot]);
+        } else {
+            ARIEL_TRY(enqueue_step(s, s->ev[slot]));
+        }
+        s->ev_pending[slot] = true;
+        // read the previous step while this one runs
+        if (s->ev_pending[slot ^ 1]) ARIEL_TRY(collect_step_events(s, slot ^ 1));
+    } else {
+        if (s->prm.use_graph && !s->graph_tried[0]) try_build_graph(s, 0);
+        if (s->graph[0]) {
+            cudaError_t e = cudaGraphLaunch(s->graph[0], s->stream);
+            if (e != cudaSuccess) return map_cuda_error(e);
+            count_launch((int)s->graph_kernels[0]);
+        } else {
+            ARIEL_TRY(enqueue_step(s, nullptr));
+        }
+    }
+    for (auto& f : s->frames) f++;
+    return ARIEL_OK;
+}
+
+ariel_status collect_pending(ariel_sim* s) {
+    // the older step first, so that the step history stays in step order
+    const int older = s->ev_slot, newer = s->ev_slot ^ 1;
+    if (s->ev_pending[older]) ARIEL_TRY(collect_step_events(s, older));
+    if (s->ev_pending[newer]) ARIEL_TRY(collect_step_events(s, newer));
+    return ARIEL_OK;
+}
+
+}  // namespace hostimpl
+}  // namespace ariel
 
 // ==============================================================================================
 // C ABI
@@ -744,6 +967,7 @@ const char* ariel_status_string(ariel_status st) {
         case ARIEL_ERR_STATE: return "call out of order";
         case ARIEL_ERR_NO_DEVICE: return "no sm_100 device";
         case ARIEL_ERR_NAN: return "non-finite input";
+        case ARIEL_ERR_PENDING: return "request not finished";
     }
     return "unknown status";
 }
@@ -758,14 +982,7 @@ ariel_status ariel_create_batch(const AsimSceneDesc* descs, int32_t k, const Asi
 
 ariel_status ariel_destroy(ariel_sim* s) {
     if (!s) return ARIEL_ERR_INVALID_ARG;
-    cudaStreamSynchronize(s->stream);
-    free_all(s);
-    for (auto& set : s->ev)
-        for (auto& e : set) cudaEventDestroy(e);
-    cudaEventDestroy(s->tb);
-    cudaEventDestroy(s->te);
-    cudaStreamDestroy(s->stream);
-    delete s;
+    delete_sim(s);
     return ARIEL_OK;
 }
 
@@ -778,19 +995,24 @@ ariel_status ariel_scene_count(ariel_sim* s, int32_t* k) {
 ariel_status ariel_init(ariel_sim* s) {
     if (!s) return ARIEL_ERR_INVALID_ARG;
     // m_max_density from the 10^3 lattice, per scene (flip.cpp:47-70)
-    k_max_density<<<s->k, 1024, 0, s->stream>>>(s->d_scenes, s->k);
-    count_launch();
-    ARIEL_CUDA(cudaGetLastError());
-    std::vector<SceneDev> dev(s->k);
-    ARIEL_CUDA(cudaMemcpyAsync(dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost, s->stream));
-    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    ARIEL_TRY(compute_max_density(s));
     for (int i = 0; i < s->k; ++i) {
-        s->sh[i].max_density = dev[i].max_density;
         s->sh[i].frame = 0;
         s->frames[i] = 0;
     }
     std::vector<HostParticles> hp(s->k);
-    for (int i = 0; i < s->k; ++i) generate_particles(s->descs[i], hp[i]);
+    {
+        // scenes are seeded independently: one host thread per scene, up to the core count
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int i = next++; i < s->k; i = next++) generate_particles(s->descs[i], hp[i]);
+        };
+        const int nt = std::max(1, std::min(s->k, (int)std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+    }
     ARIEL_TRY(build_state(s, hp));
     ARIEL_TRY(sort_and_classify_init(s));
     ARIEL_CUDA(cudaStreamSynchronize(s->stream));
@@ -805,12 +1027,7 @@ ariel_status ariel_set_particles(ariel_sim* s, int32_t scene, int64_t n, const f
     for (int64_t i = 0; i < 3 * n; ++i)
         if (!std::isfinite(pos[i]) || !std::isfinite(vel[i])) return ARIEL_ERR_NAN;
     cudaStreamSynchronize(s->stream);
-    std::vector<SceneDev> dev(s->k);
-    ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < s->k; ++i) {
-        s->sh[i].frame = dev[i].frame;
-        s->sh[i].max_density = dev[i].max_density;
-    }
+    ARIEL_TRY(refresh_scene_table(s));
     std::vector<HostParticles> hp;
     ARIEL_TRY(download_particles(s, hp));
     hp[scene].pos4.resize(n);
@@ -829,11 +1046,7 @@ ariel_status ariel_set_particles(ariel_sim* s, int32_t scene, int64_t n, const f
     ARIEL_CUDA(copy_sync(s->stream, s->S.P64, P64.data(), sizeof(double) * s->nc, cudaMemcpyHostToDevice));
     if (!s->inited) {
         // a handle fed directly with particles still needs the density normaliser
-        k_max_density<<<s->k, 1024, 0, s->stream>>>(s->d_scenes, s->k);
-        count_launch();
-        ARIEL_CUDA(cudaGetLastError());
-        ARIEL_CUDA(copy_sync(s->stream, dev.data(), s->d_scenes, sizeof(SceneDev) * s->k, cudaMemcpyDeviceToHost));
-        for (int i = 0; i < s->k; ++i) s->sh[i].max_density = dev[i].max_density;
+        ARIEL_TRY(compute_max_density(s));
         s->inited = true;
     }
     ARIEL_TRY(sort_and_classify_init(s));
@@ -854,34 +1067,8 @@ ariel_status ariel_stage(ariel_sim* s, int32_t stage) {
 ariel_status ariel_step(ariel_sim* s, int32_t nsteps) {
     if (!s || nsteps < 0) return ARIEL_ERR_INVALID_ARG;
     if (!s->inited) return ARIEL_ERR_STATE;
-    const bool timed = s->prm.timing != 0;
     for (int it = 0; it < nsteps; ++it) {
-        if (timed) {
-            const int slot = s->ev_slot;
-            s->ev_slot ^= 1;
-            if (s->ev_pending[slot]) ARIEL_TRY(collect_step_events(s, slot));
-            if (s->prm.use_graph && !s->graph_tried[1 + slot]) try_build_graph(s, 1 + slot);
-            if (s->graph[1 + slot]) {
-                cudaError_t e = cudaGraphLaunch(s->graph[1 + slot], s->stream);
-                if (e != cudaSuccess) return map_cuda_error(e);
-                count_launch((int)s->graph_kernels[1 + slot]);
-            } else {
-                ARIEL_TRY(enqueue_step(s, s->ev[slot]));
-            }
-            s->ev_pending[slot] = true;
-            // read the previous step while this one runs
-            if (s->ev_pending[slot ^ 1]) ARIEL_TRY(collect_step_events(s, slot ^ 1));
-        } else {
-            if (s->prm.use_graph && !s->graph_tried[0]) try_build_graph(s, 0);
-            if (s->graph[0]) {
-                cudaError_t e = cudaGraphLaunch(s->graph[0], s->stream);
-                if (e != cudaSuccess) return map_cuda_error(e);
-                count_launch((int)s->graph_kernels[0]);
-            } else {
-                ARIEL_TRY(enqueue_step(s, nullptr));
-            }
-        }
-        for (auto& f : s->frames) f++;
+        ARIEL_TRY(step_async(s));
         if (s->prm.fail_on_not_converged) {
             std::vector<PcgScene> sc(s->k);
             ARIEL_CUDA(cudaMemcpyAsync(sc.data(), s->PA.sc, sizeof(PcgScene) * s->k, cudaMemcpyDeviceToHost, s->stream));
@@ -894,13 +1081,8 @@ ariel_status ariel_step(ariel_sim* s, int32_t nsteps) {
                 }
         }
     }
-    if (timed) {
-        // the last step's events (its successor has not been launched)
-        for (int k2 = 0; k2 < 2; ++k2) {
-            int slot = s->ev_slot ^ 1 ^ k2;
-            if (s->ev_pending[slot]) ARIEL_TRY(collect_step_events(s, slot));
-        }
-    }
+    // the last step's events (its successor has not been launched)
+    if (s->prm.timing) ARIEL_TRY(collect_pending(s));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return map_cuda_error(e);
     return ARIEL_OK;

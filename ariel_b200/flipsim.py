@@ -219,3 +219,83 @@ class FlipSim:
     @property
     def batch(self):
         return self._b
+
+
+def state_bytes(descs, params=None):
+    """Device bytes a handle or server batch holds for these scenes."""
+    L = lib()
+    if params is None:
+        params = A.params_default()
+    arr = (A.AsimSceneDesc * len(descs))(*descs)
+    b = C.c_int64()
+    check(L.ariel_state_bytes(arr, len(descs), C.byref(params), C.byref(b)), "ariel_state_bytes")
+    return b.value
+
+
+class Server:
+    """Request server: scenes of any size arrive as (scene, steps) requests and are stepped
+    together, re-packed at step boundaries as they arrive and finish (ariel_server_*)."""
+
+    def __init__(self, params=None, hbm_budget_bytes=0, max_live=0, prepare_threads=0, keep_results=1):
+        self.L = lib()
+        if params is None:
+            params = A.params_default()
+        cfg = A.AsimServerConfig()
+        self.L.ariel_server_config_default(C.byref(cfg))
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        if max_live:
+            cfg.max_live = max_live
+        if prepare_threads:
+            cfg.prepare_threads = prepare_threads
+        cfg.keep_results = keep_results
+        h = C.c_void_p()
+        check(self.L.ariel_server_create(C.byref(params), C.byref(cfg), C.byref(h)), "ariel_server_create")
+        self.h = h
+
+    def submit(self, desc, nsteps):
+        i = C.c_int64()
+        check(self.L.ariel_server_submit(self.h, C.byref(desc), nsteps, C.byref(i)), "ariel_server_submit")
+        return i.value
+
+    def poll(self, rid):
+        info = A.AsimRequestInfo()
+        check(self.L.ariel_server_poll(self.h, rid, C.byref(info)), "ariel_server_poll")
+        return info
+
+    def wait(self, rid, timeout_ms=600000.0):
+        check(self.L.ariel_server_wait(self.h, rid, timeout_ms), "ariel_server_wait")
+
+    def drain(self, timeout_ms=600000.0):
+        check(self.L.ariel_server_drain(self.h, timeout_ms), "ariel_server_drain")
+
+    def fetch(self, rid):
+        n = self.poll(rid).n_particles
+        pos = np.zeros((n, 3), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        check(self.L.ariel_server_fetch(self.h, rid, _p(pos), _p(vel)), "ariel_server_fetch")
+        return pos, vel
+
+    def release(self, rid):
+        check(self.L.ariel_server_release(self.h, rid), "ariel_server_release")
+
+    def stats(self):
+        st = A.AsimServerStats()
+        check(self.L.ariel_server_stats(self.h, C.byref(st)), "ariel_server_stats")
+        return st
+
+    def shutdown(self):
+        if getattr(self, "h", None):
+            check(self.L.ariel_server_shutdown(self.h), "ariel_server_shutdown")
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.shutdown()
+
+    def __del__(self):
+        try:
+            self.shutdown()
+        except Exception:
+            pass

@@ -124,7 +124,7 @@ def load_traffic(workload):
         return None
 
 
-def make_params(A, precision, tol, timing=1, graph=1):
+def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
     p = A.params_default()
     p.precision = precision
     p.precond = A.PRECOND_REF
@@ -132,11 +132,13 @@ def make_params(A, precision, tol, timing=1, graph=1):
     p.tol = tol
     p.use_graph = graph
     p.timing = timing
+    p.resample_every = resample_every
     return p
 
 
 def run_gpu_pass(A, Batch, desc, prm, steps, warmup, sampler=None, barrier=None):
-    b = Batch([desc], prm)
+    descs = desc if isinstance(desc, list) else [desc]
+    b = Batch(descs, prm)
     b.init()
     b.step(warmup)
     b.synchronize()
@@ -155,36 +157,46 @@ def run_gpu_pass(A, Batch, desc, prm, steps, warmup, sampler=None, barrier=None)
         clocks = None
     launches = b.L.ariel_kernel_launches() - launches0
     tim = b.timing(max_steps=steps)
-    tot = b.solver_totals()
+    tots = [b.solver_totals(i) for i in range(b.k)]
+    tot = tots[0]
+    if b.k > 1:
+        # batch totals: solves are simultaneous, so count one solve per step
+        for name in ("iterations", "outer", "cell_iterations", "cell_outer", "not_converged"):
+            setattr(tot, name, sum(getattr(t, name) for t in tots))
+        tot.solves = tots[0].solves
     st = b.stats()
     return b, dict(ms=ms, timing=tim, totals=tot, stats=st, clocks=clocks, launches=launches,
-                   np=b.count())
+                   np=sum(b.count(i) for i in range(b.k)))
 
 
 def run_e2e(b, steps):
     """Same metric through the public API with host buffers: every step uploads the particle
-    state from pinned host memory, steps, and reads the new state back."""
+    state of every scene from pinned host memory, steps, and reads the new state back."""
     import numpy as np
-    n = b.count()
-    try:
-        import torch
-        pos_t = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        vel_t = torch.empty((n, 3), dtype=torch.float32, pin_memory=True)
-        pos, vel = pos_t.numpy(), vel_t.numpy()
-        pinned = True
-    except Exception:
-        pos = np.empty((n, 3), np.float32)
-        vel = np.empty((n, 3), np.float32)
-        pinned = False
-    b.download_state(pos, vel)
+    bufs, pinned, total = [], True, 0
+    for i in range(b.k):
+        n = b.count(i)
+        total += n
+        try:
+            import torch
+            pos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+            vel = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        except Exception:
+            pos = np.empty((n, 3), np.float32)
+            vel = np.empty((n, 3), np.float32)
+            pinned = False
+        b.download_state(pos, vel, i)
+        bufs.append((pos, vel))
     b.synchronize()
     b.timer_begin()
     for _ in range(steps):
-        b.upload_state(pos, vel)
+        for i, (pos, vel) in enumerate(bufs):
+            b.upload_state(pos, vel, i)
         b.step(1)
-        b.download_state(pos, vel)
+        for i, (pos, vel) in enumerate(bufs):
+            b.download_state(pos, vel, i)
     ms = b.timer_end()
-    return ms, 24 * n, 24 * n, pinned
+    return ms, 24 * total, 24 * total, pinned
 
 
 def cpu_baseline_sample(A, desc, tol, faithful=True, max_steps=1):
@@ -242,12 +254,94 @@ def reference_arm(args, A, ws, rank):
 
 
 def config_dict(args, n_particles, ws):
+    if args.workload == "batch":
+        return {"workload": "batched: %d dam-break scenes, grids drawn from {32,48,64,96,128}^3 (seed %d), "
+                            "blocks filling 20-50%% of each domain, %d particles in all, %s PCG to %g relative "
+                            "residual, one launch per stage over all scenes" % (args.scenes, args.seed, n_particles,
+                                                                               args.precision, args.tol),
+                "scenes": args.scenes, "seed": args.seed, "particles": n_particles, "precision": args.precision,
+                "tolerance": args.tol, "parallelism": "replicas" if ws > 1 else "single",
+                "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
+    if args.workload == "sphere":
+        return {"workload": "dam break %d^3 with a static solid sphere (c=(.6,.3,.5), r=.15), %d particles, "
+                            "dt 1/480, resampling every 5 steps, %s PCG to %g relative residual"
+                            % (args.n, n_particles, args.precision, args.tol),
+                "grid": args.n, "particles_per_scene": n_particles, "precision": args.precision,
+                "tolerance": args.tol, "parallelism": "replicas" if ws > 1 else "single",
+                "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
     return {"workload": "dam break %d^3, %d particles per scene, mixed-precision PCG to %g relative residual"
             % (args.n, n_particles, args.tol),
             "grid": args.n, "particles_per_scene": n_particles, "scenes": ws, "precision": args.precision,
             "preconditioner": "reference (solver.inl:104-135)", "tolerance": args.tol, "dt": 1.0 / 240.0,
             "parallelism": "replicas" if ws > 1 else "single",
             "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
+
+
+def serve_arm(args, A, prec, ws, rank, pg, gpu_index):
+    """Poisson arrivals through the request server for `duration` seconds.  `value` is the
+    particle-steps the server ran in that window divided by its length; the step latency
+    percentiles are device times of the batch steps."""
+    from ariel_b200 import workloads as W
+    from ariel_b200.flipsim import Server
+    stream = W.arrival_stream(args.rate, args.duration, seed=args.seed + 1000 * rank)
+    prm = make_params(A, prec, args.tol)
+    srv = Server(prm, max_live=args.max_live, keep_results=0)
+    sampler = ClockSampler(gpu_index)
+    if pg:
+        pg.barrier()
+    sampler.start()
+    t0 = time.perf_counter()
+    launches0 = srv.L.ariel_kernel_launches()
+    st0 = srv.stats()
+    for ta, d in stream:
+        dt = t0 + ta - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        srv.submit(d, args.serve_steps)
+    dt = t0 + args.duration - time.perf_counter()
+    if dt > 0:
+        time.sleep(dt)
+    st = srv.stats()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    launches = srv.L.ariel_kernel_launches() - launches0
+    srv.shutdown()
+    ps = st.particle_steps - st0.particle_steps
+    from ariel_b200.replicas import aggregate
+    # replicas: every rank serves its own stream; the job's window is the longest rank's
+    ms, ps_all = aggregate(wall * 1000.0, ps, pg)
+    value = ps_all / (ms / 1000.0)
+    out = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+        "steps": int(st.batch_steps), "warmup": 0, "ms_per_step": st.step_ms_p50,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals (mean %g/s) of dam-break scenes with grids uniform "
+                               "in 48^3-192^3 and blocks filling 20-50%%, %d steps each, %s PCG to %g, admitted "
+                               "by device-byte budget, at most %d live, over %.0f s"
+                               % (args.rate, args.serve_steps, args.precision, args.tol, args.max_live, args.duration),
+                   "rate": args.rate, "duration_s": args.duration, "steps_per_request": args.serve_steps,
+                   "max_live": args.max_live, "precision": args.precision,
+                   "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "inputs larger than L2"},
+        "serving": {"submitted": len(stream), "admitted": st.admitted, "finished": st.finished,
+                    "failed": st.failed, "live_at_end": st.live, "waiting_at_end": st.waiting,
+                    "batch_steps": st.batch_steps, "particle_steps": ps, "busy_frac": st.busy_ms / (wall * 1000.0),
+                    "step_ms_p50": st.step_ms_p50, "step_ms_p99": st.step_ms_p99, "step_ms_max": st.step_ms_max,
+                    "request_latency_ms_p50": st.latency_ms_p50 if st.finished else None,
+                    "request_latency_ms_p99": st.latency_ms_p99 if st.finished else None,
+                    "relayouts": st.relayouts, "relayout_ms": st.relayout_ms,
+                    "hbm_budget_gb": st.hbm_budget_bytes / 1e9, "hbm_peak_gb": st.hbm_peak_bytes / 1e9,
+                    "max_live_seen": st.max_live_seen},
+        "step_ms_p50": st.step_ms_p50, "step_ms_p99": st.step_ms_p99,
+        "clocks": clocks, "gpu_launches": launches,
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "api": "ariel_server_submit (host-seeded scenes, results copied out at retirement)",
+                "note": "the server path is end to end by construction: scenes enter from the host and leave "
+                        "to host memory; inputs are uploaded once per request, not per step"},
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
 
 
 def main():
@@ -263,7 +357,18 @@ def main():
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget-s", type=float, default=150.0)
+    ap.add_argument("--workload", choices=["dambreak", "sphere", "batch", "serve"], default="dambreak",
+                    help="dambreak: the headline 128^3 scene; sphere: 256^3 with a solid sphere; batch: 64 "
+                         "uneven scenes stepped together; serve: Poisson arrivals through the request server")
+    ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
+    ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
+    ap.add_argument("--serve-steps", type=int, default=200)
+    ap.add_argument("--max-live", type=int, default=32)
     args = ap.parse_args()
+    if args.workload == "sphere" and args.n == 128:
+        args.n = 256
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
 
@@ -287,10 +392,25 @@ def main():
         return rc
 
     prec = {"mixed": A.PREC_MIXED, "fp64": A.PREC_FP64, "ref32": A.PREC_REF32}[args.precision]
-    desc = A.scene_dambreak(args.n, seed=replica_seed(rank))
+    from ariel_b200 import workloads as W
+    resample_every = 1
+    if args.workload == "serve":
+        rc = serve_arm(args, A, prec, ws, rank, pg, gpu_index)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return rc
+    if args.workload == "batch":
+        desc = W.uneven_batch(args.scenes, seed=args.seed + 1000 * rank)
+    elif args.workload == "sphere":
+        desc = W.sphere_dambreak(args.n, seed=replica_seed(rank))
+        resample_every = 5
+    else:
+        desc = A.scene_dambreak(args.n, seed=replica_seed(rank))
     barrier = (lambda: pg.barrier()) if pg else None
     sampler = ClockSampler(gpu_index)
-    b, res = run_gpu_pass(A, Batch, desc, make_params(A, prec, args.tol), args.steps, args.warmup, sampler, barrier)
+    b, res = run_gpu_pass(A, Batch, desc, make_params(A, prec, args.tol, resample_every=resample_every),
+                          args.steps, args.warmup, sampler, barrier)
 
     n_local = res["np"]
     ms, total_particles = aggregate(res["ms"], n_local, pg)
@@ -339,7 +459,8 @@ def main():
     b.close()
 
     if not args.no_fp64_compare and args.precision != "fp64":
-        b64, r64 = run_gpu_pass(A, Batch, desc, make_params(A, A.PREC_FP64, args.tol), args.steps, args.warmup)
+        b64, r64 = run_gpu_pass(A, Batch, desc, make_params(A, A.PREC_FP64, args.tol, resample_every=resample_every),
+                                args.steps, args.warmup)
         b64.close()
         t64 = r64["totals"]
         solve64 = r64["timing"]["solve_kernel_ms"] / max(t64.solves, 1)
@@ -349,7 +470,7 @@ def main():
         # per-GPU ratio of this rank's mixed pass to its plain FP64 pass
         out["throughput_vs_fp64"] = r64["ms"] / res["ms"] if res["ms"] > 0 else None
 
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "dambreak":
         n, dt, cores, st = cpu_baseline_sample(A, desc, args.tol)
         out["cpu_baseline"] = {"value": n / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
                                "sample": "1 FLIP step (from Init) of the same %d^3 dam break, %d particles, "

@@ -44,7 +44,8 @@ typedef enum ariel_status {
     ARIEL_ERR_CUDA = 5,           /* a CUDA runtime call failed */
     ARIEL_ERR_STATE = 6,          /* call out of order (e.g. step before init) */
     ARIEL_ERR_NO_DEVICE = 7,      /* no usable sm_100 device */
-    ARIEL_ERR_NAN = 8             /* non-finite value in host input */
+    ARIEL_ERR_NAN = 8,            /* non-finite value in host input */
+    ARIEL_ERR_PENDING = 9         /* server request not finished within the wait */
 } ariel_status;
 
 /* Cell types: enum geomtype {SOLID=2, FLUID=1, AIR=0} (src/grid/macgrid.inl:13). */
@@ -280,6 +281,75 @@ const char* ariel_last_error(void);
  * overlap on the GPU race and must be serialised by the caller. */
 ariel_status ariel_sort_by_cell_noalloc(const float* pos, int64_t n, int32_t dim, uint32_t* particle_cell,
                                         uint32_t* cell_start, uint32_t* order, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Request server (continuous batching).  No counterpart in the reference, whose viewer steps one
+ * scene in a loop (src/viewer/viewer.cpp:66-87).  Scenes arrive as requests of a number of
+ * steps; host threads seed their particles while the device steps the live ones; between two
+ * batch steps the server retires finished scenes (copying their particles out) and admits
+ * waiting ones, oldest first, while the device bytes of the re-packed layout fit the budget.
+ * All live scenes share each stage's launch.  A scene's results are the same as when it is
+ * stepped alone with the same AsimParams.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct ariel_server ariel_server;
+
+typedef struct AsimServerConfig {
+    int64_t hbm_budget_bytes; /* device bytes for scene state; 0: 85% of the free memory */
+    int32_t max_live;         /* scenes stepped together at most (<= 1024); 0: 32 */
+    int32_t prepare_threads;  /* host threads seeding arriving scenes; 0: 4 */
+    int32_t keep_results;     /* 1: keep each finished scene's particles for fetch */
+    int32_t reserved[7];
+} AsimServerConfig;
+
+enum { ARIEL_REQ_QUEUED = 0, ARIEL_REQ_READY = 1, ARIEL_REQ_RUNNING = 2, ARIEL_REQ_DONE = 3, ARIEL_REQ_FAILED = 4 };
+
+typedef struct AsimRequestInfo {
+    int32_t state;        /* ARIEL_REQ_* */
+    int32_t status;       /* failure status when FAILED */
+    int32_t nsteps;
+    int32_t steps_done;   /* steps queued for this scene so far */
+    int64_t n_particles;  /* known once seeded */
+    int64_t state_bytes;  /* device bytes of the scene alone */
+    double submit_ms, admit_ms, done_ms; /* since server creation; -1 until reached */
+    AsimStats stats;      /* the scene's stats after its last step (DONE) */
+} AsimRequestInfo;
+
+typedef struct AsimServerStats {
+    int64_t submitted, admitted, finished, failed, live, waiting;
+    int64_t batch_steps;      /* steps of the whole batch */
+    int64_t particle_steps;   /* sum over batch steps of the particles stepped */
+    int64_t timed_steps;      /* batch steps with a device time below */
+    double wall_ms;           /* since server creation */
+    double busy_ms;           /* device time of all batch steps */
+    double step_ms_p50, step_ms_p99, step_ms_max; /* device time per batch step */
+    double latency_ms_p50, latency_ms_p99;        /* submit -> done per finished request */
+    int64_t relayouts;
+    double relayout_ms;       /* host time spent re-packing (includes admission copies) */
+    int64_t hbm_budget_bytes, hbm_in_use_bytes, hbm_peak_bytes;
+    int32_t max_live_seen;
+    int32_t last_error;
+} AsimServerStats;
+
+void ariel_server_config_default(AsimServerConfig* config);
+ariel_status ariel_server_create(const AsimParams* params, const AsimServerConfig* config, ariel_server** out);
+/* Queues a scene for `nsteps` steps; returns at once with its id. */
+ariel_status ariel_server_submit(ariel_server* server, const AsimSceneDesc* desc, int32_t nsteps, int64_t* id);
+ariel_status ariel_server_poll(ariel_server* server, int64_t id, AsimRequestInfo* info);
+/* ARIEL_OK when the request is done, its failure status when it failed, ARIEL_ERR_PENDING
+ * when `timeout_ms` passed first. */
+ariel_status ariel_server_wait(ariel_server* server, int64_t id, double timeout_ms);
+/* Waits until every submitted request is done or failed (ARIEL_ERR_PENDING on timeout). */
+ariel_status ariel_server_drain(ariel_server* server, double timeout_ms);
+/* A finished request's particles, id order, xyz-interleaved (3 * n_particles floats each). */
+ariel_status ariel_server_fetch(ariel_server* server, int64_t id, float* pos, float* vel);
+/* Forgets a finished request and its results. */
+ariel_status ariel_server_release(ariel_server* server, int64_t id);
+ariel_status ariel_server_stats(ariel_server* server, AsimServerStats* stats);
+/* Stops the server; requests not finished fail with ARIEL_ERR_STATE.  Frees the handle. */
+ariel_status ariel_server_shutdown(ariel_server* server);
+/* Device bytes a handle (or a server batch) holds for these scenes (seeds them on the host to
+ * count their particles). */
+ariel_status ariel_state_bytes(const AsimSceneDesc* descs, int32_t k, const AsimParams* params, int64_t* bytes);
 
 #ifdef __cplusplus
 }

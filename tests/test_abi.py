@@ -42,7 +42,7 @@ def test_defaults_match_reference_constants():
 
 def test_status_strings():
     L = _lib.lib()
-    for code in range(9):
+    for code in range(10):
         assert L.ariel_status_string(code)
 
 
