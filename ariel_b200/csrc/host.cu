@@ -204,6 +204,7 @@ long long layout_bytes(const Layout& L) {
     add(1, 4);       // dev_error
     add((long long)scan_tmp_bytes(nc), 1);
     add(nc, 4);      // FLUID list
+    add(nc, 16);     // FLUID-list records
     add(k + 1, 8);
     add(k + 1, 8);
     add(nc, 4);      // flpred
@@ -531,6 +532,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     ARIEL_TRY(dalloc(s, &flp, k + 1));
     ARIEL_TRY(dalloc(s, &chp, k + 1));
     A.fl = fl;
+    ARIEL_TRY(dalloc(s, &A.rec, nc));
     A.fl_pref = flp;
     A.ch_pref = chp;
     ARIEL_TRY(dalloc(s, &s->flpred, nc));
@@ -568,6 +570,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     ARIEL_TRY(dalloc(s, &S.solid_pos, s->spref[k], true));
     A.S = S;
     s->pcg_blocks = pcg_max_blocks(s->device, s->mode, s->prm.pcg_blocks_per_sm);
+    if (s->prm.pcg_grid_blocks > 0) s->pcg_blocks = std::min(s->pcg_blocks, (int)s->prm.pcg_grid_blocks);
     cudaStream_t st = s->stream;
     // scene table and prefixes
     ARIEL_CUDA(cudaMemcpyAsync(s->d_scenes, s->sh.data(), sizeof(SceneDev) * k, cudaMemcpyHostToDevice, st));

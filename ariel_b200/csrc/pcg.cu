@@ -242,10 +242,27 @@ __global__ void k_prep_cells(PcgArgs A, uint32_t* pred) {
     if (one) atomicAdd(&A.sc[s].ones, 1);
 }
 
+// FLUID list, plus one 16-byte record per entry holding everything the solve needs about the
+// cell besides its vectors: index, neighbour mask and ADiag (fp32 bits for the fp32 modes, fp64
+// bits otherwise), so that a single load starts a cell's update.
 __global__ void k_fl_write(PcgArgs A, const uint32_t* pred, const uint32_t* scan) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= A.S.nc) return;
-    if (pred[c]) const_cast<uint32_t*>(A.fl)[scan[c]] = (uint32_t)c;
+    if (!pred[c]) return;
+    const uint32_t t = scan[c];
+    const_cast<uint32_t*>(A.fl)[t] = (uint32_t)c;
+    uint4 r;
+    r.x = (uint32_t)c;
+    r.y = (uint32_t)A.mask[c];
+    if (A.mode == kFp64) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(A.diag[c]);
+        r.z = (uint32_t)b;
+        r.w = (uint32_t)(b >> 32);
+    } else {
+        r.z = __float_as_uint((float)A.diag[c]);
+        r.w = 0u;
+    }
+    A.rec[t] = r;
 }
 
 __global__ void k_pcg_tables(PcgArgs A, const uint32_t* scan) {
@@ -1222,6 +1239,13 @@ __device__ __forceinline__ double4 mk4<double>(double a, double b, double c, dou
     return make_double4(a, b, c, d);
 }
 
+__device__ __forceinline__ void dec_diag(const uint4& r, float& d) { d = __uint_as_float(r.z); }
+__device__ __forceinline__ void dec_diag(const uint4& r, double& d) {
+    d = __longlong_as_double((long long)(((unsigned long long)r.w << 32) | (unsigned long long)r.z));
+}
+
+// Dynamic shared memory of k_pcg_fast: the per-solve caches of the block's first chunks
+// (diagonal, cell index, mask).
 size_t fast_dyn_smem(int mode) {
     const size_t tb = mode == kFp64 ? 8 : 4;
     return (size_t)kFlCacheChunks * kChunkCells * (4 + 1 + tb);
@@ -1260,9 +1284,41 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     double* part2 = A.partial + 2 * MC;
     const unsigned long long tmo = A.timeout_ns;
     unsigned epoch = 0;
+    // Chunk sums are reduced per warp at once but combined across warps only every kDefer
+    // chunks (and at the end of each pass), so warps never wait for one another inside a pass.
+    // The combination is the same fixed tree as block_sum2: lane-0 warp sums, then one warp
+    // over the warp sums with zero padding.
+    constexpr int kDefer = 16;
+    constexpr int kWarps = kPcgThreads / 32;
+    __shared__ double dsum[kDefer][3][kWarps];
+    int npend = 0, jpend0 = 0;
+    auto flush = [&]() {
+        if (npend == 0) return;
+        __syncthreads();
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        for (int jj = wid; jj < npend; jj += kWarps) {
+            double v0 = lane < kWarps ? dsum[jj][0][lane] : 0.0;
+            double v1 = lane < kWarps ? dsum[jj][1][lane] : 0.0;
+            double v2 = lane < kWarps ? dsum[jj][2][lane] : 0.0;
+            v0 = warp_sum(v0);
+            v1 = warp_sum(v1);
+            v2 = warp_sum(v2);
+            if (lane == 0) {
+                const long long ch = blockIdx.x + (long long)(jpend0 + jj) * gridDim.x;
+                part0[ch] = v0;
+                part1[ch] = v1;
+                part2[ch] = v2;
+            }
+        }
+        __syncthreads();
+        npend = 0;
+    };
     auto chunk_of = [&](int j, int& s, long long& t0, long long& t1) -> bool {
         long long ch = blockIdx.x + (long long)j * gridDim.x;
-        if (ch >= nch) return false;
+        if (ch >= nch) {
+            flush();  // every chunk pass ends here
+            return false;
+        }
         s = find_scene(ch_s, k, ch);
         t0 = fl_s[s] + (ch - ch_s[s]) * kChunkCells;
         t1 = min(t0 + (long long)kChunkCells, fl_s[s + 1]);
@@ -1273,11 +1329,13 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
         long long t0, t1;
         if (!chunk_of(j, s, t0, t1)) break;
         for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-            uint32_t c = A.fl[t];
+            const uint4 rc = A.rec[t];
             int o = j * kChunkCells + (int)(t - t0);
-            flc[o] = c;
-            mkc[o] = A.mask[c];
-            dgc[o] = (T)A.diag[c];
+            flc[o] = rc.x;
+            mkc[o] = (uint8_t)rc.y;
+            T dg;
+            dec_diag(rc, dg);
+            dgc[o] = dg;
         }
     }
     __syncthreads();
@@ -1290,16 +1348,32 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     auto diag_at = [&](int j, long long t, long long t0, long long c) -> T {
         return j < kFlCacheChunks ? dgc[j * kChunkCells + (int)(t - t0)] : (T)A.diag[c];
     };
-    auto put3 = [&](int j, double a, double b, double c) {
-        double z0 = 0.0;
-        block_sum2(a, b);
-        block_sum2(c, z0);
-        if (threadIdx.x == 0) {
-            long long ch = blockIdx.x + (long long)j * gridDim.x;
-            part0[ch] = a;
-            part1[ch] = b;
-            part2[ch] = c;
+    // cell, mask and diagonal of list entry t from one shared-memory or one 16-byte global read
+    auto cell_rec = [&](int j, long long t, long long t0, long long& c, uint32_t& m, T& dg) {
+        if (j < kFlCacheChunks) {
+            const int o = j * kChunkCells + (int)(t - t0);
+            c = (long long)flc[o];
+            m = (uint32_t)mkc[o];
+            dg = dgc[o];
+        } else {
+            const uint4 rc = A.rec[t];
+            c = (long long)rc.x;
+            m = rc.y;
+            dec_diag(rc, dg);
         }
+    };
+    auto put3 = [&](int j, double a, double b, double c) {
+        a = warp_sum(a);
+        b = warp_sum(b);
+        c = warp_sum(c);
+        if (npend == 0) jpend0 = j;
+        if ((threadIdx.x & 31) == 0) {
+            const int wid = threadIdx.x >> 5;
+            dsum[npend][0][wid] = a;
+            dsum[npend][1][wid] = b;
+            dsum[npend][2][wid] = c;
+        }
+        if (++npend == kDefer) flush();
     };
     auto reduce = [&](int nsum, auto&& f) {
         if (threadIdx.x == 0) s_active = 0;
@@ -1465,38 +1539,62 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         const T bt = (T)L[s].beta;
                         const T scale = (T)(1.0 / (double)D.ax_h);
                         const long long nn = (long long)D.n * D.n, n1 = D.n;
-                        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-                            const long long c = cell_at(j, t, t0);
-                            const uint32_t m = mask_at(j, t, t0, c);
-                            const T dg = diag_at(j, t, t0, c);
-                            // all loads first: own state and the six neighbours' (r, w, s, pc)
-                            const T4 a = ld4(Ac + c);
-                            const T4 b = ld4(Bv + c);
-                            T4 nb[6];
-                            const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
+                        // kIlp list entries per thread at once (t, t + blockDim.x, ...): their
+                        // loads overlap; the sums still accumulate in ascending t per thread.
+                        constexpr int kIlp = MODE == kFp64 ? 1 : 2;
+                        const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
+                        for (long long tb = t0 + threadIdx.x; tb < t1; tb += (long long)kIlp * blockDim.x) {
+                            long long c[kIlp];
+                            uint32_t m[kIlp];
+                            T dg[kIlp];
+                            bool on[kIlp];
 #pragma unroll
-                            for (int d = 0; d < 6; ++d) nb[d] = ld4(Ac + ((m >> d) & 1u ? c + off[d] : c));
-                            const T sv = it == 0 ? a.y : a.y + bt * a.z;
-                            const T pvv = it == 0 ? b.x : b.x + bt * b.y;
-                            const T xv = b.z + al * pvv;
-                            const T rn = a.x - al * sv;
-                            const T un = (rn * a.w) * a.w;
-                            T acc = dg * un;
-#pragma unroll
-                            for (int d = 0; d < 6; ++d) {
-                                if ((m >> d) & 1u) {
-                                    const T4 e = nb[d];
-                                    const T sq = it == 0 ? e.y : e.y + bt * e.z;
-                                    const T rq = e.x - al * sq;
-                                    acc -= (rq * e.w) * e.w;
+                            for (int u = 0; u < kIlp; ++u) {
+                                const long long t = tb + (long long)u * blockDim.x;
+                                on[u] = t < t1;
+                                if (on[u]) {
+                                    cell_rec(j, t, t0, c[u], m[u], dg[u]);
+                                } else {
+                                    c[u] = c[0];
+                                    m[u] = 0u;
+                                    dg[u] = (T)0;
                                 }
                             }
-                            const T wn = acc * scale;
-                            st4(An + c, mk4<T>(rn, wn, sv, a.w));
-                            st4(Bv + c, mk4<T>(un, pvv, xv, (T)0));
-                            g1 += (double)rn * (double)un;
-                            d1 += (double)wn * (double)un;
-                            q1 += (double)rn * (double)rn;
+                            // all loads first: own state and the six neighbours' (r, w, s, pc)
+                            T4 a[kIlp], b[kIlp], nb[kIlp][6];
+#pragma unroll
+                            for (int u = 0; u < kIlp; ++u) {
+                                a[u] = ld4(Ac + c[u]);
+                                b[u] = ld4(Bv + c[u]);
+#pragma unroll
+                                for (int d = 0; d < 6; ++d)
+                                    nb[u][d] = ld4(Ac + ((m[u] >> d) & 1u ? c[u] + off[d] : c[u]));
+                            }
+#pragma unroll
+                            for (int u = 0; u < kIlp; ++u) {
+                                if (!on[u]) continue;
+                                const T sv = it == 0 ? a[u].y : a[u].y + bt * a[u].z;
+                                const T pvv = it == 0 ? b[u].x : b[u].x + bt * b[u].y;
+                                const T xv = b[u].z + al * pvv;
+                                const T rn = a[u].x - al * sv;
+                                const T un = (rn * a[u].w) * a[u].w;
+                                T acc = dg[u] * un;
+#pragma unroll
+                                for (int d = 0; d < 6; ++d) {
+                                    if ((m[u] >> d) & 1u) {
+                                        const T4 e = nb[u][d];
+                                        const T sq = it == 0 ? e.y : e.y + bt * e.z;
+                                        const T rq = e.x - al * sq;
+                                        acc -= (rq * e.w) * e.w;
+                                    }
+                                }
+                                const T wn = acc * scale;
+                                st4(An + c[u], mk4<T>(rn, wn, sv, a[u].w));
+                                st4(Bv + c[u], mk4<T>(un, pvv, xv, (T)0));
+                                g1 += (double)rn * (double)un;
+                                d1 += (double)wn * (double)un;
+                                q1 += (double)rn * (double)rn;
+                            }
                         }
                     }
                     put3(j, g1, d1, q1);

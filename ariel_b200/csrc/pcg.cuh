@@ -65,6 +65,7 @@ struct PcgArgs {
     unsigned long long timeout_ns;
     // FLUID list
     const uint32_t* fl;        // packed FLUID cells, scene by scene, ascending
+    uint4* rec;                // per FLUID-list entry: (cell, neighbour mask, diagonal bits)
     const long long* fl_pref;  // k+1
     const long long* ch_pref;  // k+1 chunk begins
     // per-cell operator data (dense over packed cells)

@@ -157,6 +157,8 @@ typedef struct AsimParams {
     int32_t fail_on_not_converged; /* return ARIEL_ERR_NOT_CONVERGED from step when a solve
                                       stops at max_iters above tolerance */
     int32_t pcg_blocks_per_sm;  /* blocks per SM of the persistent solve kernel; 0 = default (2) */
+    int32_t pcg_grid_blocks;    /* >0: cap on the solve kernel's blocks in all (results do not
+                                   depend on it; tests and tuning); 0 = one grid of resident blocks */
 } AsimParams;
 
 typedef struct AsimStats {

@@ -149,3 +149,19 @@ def test_mic0_against_oracle(precision):
     err = np.linalg.norm((mic["P64"] - xstar)[fl]) / np.linalg.norm(xstar[fl])
     assert err < 1e-4
     assert mic["stats"].pcg_iterations < ref["stats"].pcg_iterations
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED, A.PREC_REF32])
+def test_solve_independent_of_grid_size(precision):
+    """One block (which then works through chunks beyond its shared-memory cache, reading the
+    packed per-entry records) gives the same bits as the default grid: every chunk's partial
+    sums and the tree over chunks are fixed by the FLUID list alone."""
+    desc, st, g = _solve_inputs(32)
+    assert (g["A"] == A.FLUID).sum() > 5 * 1024  # more chunks than one block caches
+    runs = [_gpu_solve(desc, st, g, params(precision=precision, stop=A.STOP_REL, tol=1e-6, pcg_grid_blocks=nb))
+            for nb in (0, 1)]
+    for key in ("P", "P64"):
+        assert np.array_equal(runs[0][key].view(np.uint8), runs[1][key].view(np.uint8)), key
+    assert runs[0]["stats"].pcg_iterations == runs[1]["stats"].pcg_iterations
+    assert runs[0]["stats"].pcg_converged == 1
