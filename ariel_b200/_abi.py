@@ -69,7 +69,7 @@ class AsimParams(C.Structure):
         ("resample_every", C.c_int32), ("mic_tau", C.c_double), ("mic_sigma", C.c_double),
         ("rng_seed", C.c_uint64), ("use_graph", C.c_int32), ("timing", C.c_int32),
         ("barrier_timeout_ms", C.c_double), ("fail_on_not_converged", C.c_int32),
-        ("pcg_blocks_per_sm", C.c_int32), ("pcg_grid_blocks", C.c_int32),
+        ("pcg_blocks_per_sm", C.c_int32), ("pcg_grid_blocks", C.c_int32), ("sweep_brick", C.c_int32 * 3),
     ]
 
 

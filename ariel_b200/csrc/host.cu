@@ -154,10 +154,26 @@ void free_all(ariel_sim* s) { free_bufs(s, false); }
 
 // Buffer sizes of one packed layout.
 struct Layout {
-    long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0;
+    long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0, nbricks = 0;
     bool any_solid = false;
     int mode = kRef32;
 };
+
+// Brick of the ordered wavefront sweeps.
+void sweep_brick(const AsimParams& p, int& bx, int& by, int& bz) {
+    bx = p.sweep_brick[0];
+    by = p.sweep_brick[1];
+    bz = p.sweep_brick[2];
+    if (bx == 0 && by == 0 && bz == 0) {
+        bx = 8;
+        by = 16;
+        bz = 16;
+    }
+}
+
+long long bricks_of(int n, int bx, int by, int bz) {
+    return (long long)((n + bx - 1) / bx) * ((n + by - 1) / by) * ((n + bz - 1) / bz);
+}
 
 int mode_of(const AsimParams& p) {
     return p.precision == ARIEL_PREC_FP64 ? kFp64 : (p.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
@@ -221,6 +237,9 @@ long long layout_bytes(const Layout& L) {
         add(nc, 4);
     }
     add(3 * std::max(1ll, L.maxch), 8);
+    add(L.nbricks, 16);  // brick list
+    add(k + 1, 4);       // brick bases
+    add(L.nbricks, 4);   // brick flags
     add(k, sizeof(PcgScene));
     add(k, sizeof(PcgTotals));
     add(1, sizeof(PcgCtl));
@@ -406,8 +425,11 @@ long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector
     Layout L;
     L.k = (long long)descs.size();
     L.mode = mode_of(prm);
+    int bx, by, bz;
+    sweep_brick(prm, bx, by, bz);
     for (size_t i = 0; i < descs.size(); ++i) {
         const long long n = descs[i].dim;
+        L.nbricks += bricks_of((int)n, bx, by, bz);
         L.np += particles[i];
         L.nc += n * n * n;
         L.nf += 3 * n * n * (n + 1);
@@ -563,6 +585,29 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     }
     A.max_chunks = std::max(1ll, maxch);
     ARIEL_TRY(dalloc(s, &A.partial, 3 * A.max_chunks));
+    // bricks of the ordered sweeps: every scene's brick grid, listed by level I+J+K, then scene
+    // and position (the order the sweeps take them in)
+    sweep_brick(s->prm, A.bx, A.by, A.bz);
+    std::vector<int4> bricks;
+    std::vector<int> bbase(k + 1, 0);
+    for (int i = 0; i < k; ++i) {
+        const int n = s->descs[i].dim;
+        const int nbI = (n + A.bx - 1) / A.bx, nbJ = (n + A.by - 1) / A.by, nbK = (n + A.bz - 1) / A.bz;
+        bbase[i + 1] = bbase[i] + nbI * nbJ * nbK;
+        for (int I = 0; I < nbI; ++I)
+            for (int J = 0; J < nbJ; ++J)
+                for (int K = 0; K < nbK; ++K) bricks.push_back(make_int4(i, I, J, K));
+    }
+    std::stable_sort(bricks.begin(), bricks.end(),
+                     [](const int4& a, const int4& b) { return a.y + a.z + a.w < b.y + b.z + b.w; });
+    A.nbricks = (int)bricks.size();
+    int4* dbr = nullptr;
+    int* dbase = nullptr;
+    ARIEL_TRY(dalloc(s, &dbr, bricks.size()));
+    ARIEL_TRY(dalloc(s, &dbase, (size_t)k + 1));
+    ARIEL_TRY(dalloc(s, &A.bflag, bricks.size()));
+    A.bricks = dbr;
+    A.brick_base = dbase;
     ARIEL_TRY(dalloc(s, &A.sc, k, true));
     ARIEL_TRY(dalloc(s, &A.totals, k, true));
     ARIEL_TRY(dalloc(s, &A.ctl, 1));
@@ -584,6 +629,9 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     ARIEL_CUDA(cudaMemsetAsync(S.pu, 0, sizeof(float) * nf, st));
     ARIEL_CUDA(cudaMemsetAsync(S.flags, 0, nc, st));
     ARIEL_CUDA(cudaMemsetAsync(A.sc, 0, sizeof(PcgScene) * k, st));
+    if (!bricks.empty())
+        ARIEL_CUDA(copy_sync(st, dbr, bricks.data(), bricks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    ARIEL_CUDA(copy_sync(st, dbase, bbase.data(), bbase.size() * sizeof(int), cudaMemcpyHostToDevice));
     ARIEL_CUDA(cudaMemsetAsync(A.totals, 0, sizeof(PcgTotals) * k, st));
     // per-scene persistent state
     uint32_t* stage_u32 = nullptr;
@@ -833,6 +881,9 @@ ariel_status check_params(const AsimParams* params) {
     if (params->precision < 0 || params->precision > 2 || params->precond < 0 || params->precond > 1 ||
         params->stop_rule < 0 || params->stop_rule > 1)
         return ARIEL_ERR_INVALID_ARG;
+    int bx, by, bz;
+    sweep_brick(*params, bx, by, bz);
+    if (!brick_shape_ok(bx, by, bz)) return ARIEL_ERR_INVALID_ARG;
     return ARIEL_OK;
 }
 

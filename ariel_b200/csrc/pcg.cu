@@ -288,166 +288,325 @@ __global__ void k_pcg_tables(PcgArgs A, const uint32_t* scan) {
     A.ctl->any_ordered = any_ordered;
 }
 
-// ------------------------------------------------------------------------------------------
-// Ordered preconditioner: one block sweeps a scene's i+j+k hyperplanes (forward) or in
-// reverse (backward); cells of one plane are independent.
-// ------------------------------------------------------------------------------------------
-template <class F>
-__device__ void hyperplanes(int n, bool reverse, F&& f) {
-    const int nd = 3 * (n - 1) + 1;
-    for (int di = 0; di < nd; ++di) {
-        const int d = reverse ? nd - 1 - di : di;
-        const int ilo = max(0, d - 2 * (n - 1)), ihi = min(n - 1, d);
-        const long long cnt = (long long)(ihi - ilo + 1) * n;
-        for (long long idx = threadIdx.x; idx < cnt; idx += blockDim.x) {
-            int i = ilo + (int)(idx / n), j = (int)(idx % n);
-            int k = d - i - j;
-            if (k >= 0 && k < n) f(i, j, k);
-        }
-        __threadfence_block();
-        __syncthreads();
-    }
-}
-
 // Data written by other blocks is read only after a grid barrier (whose acquire makes ordinary
-// loads observe it) or, inside an ordered sweep, after __syncthreads of the writing block.
+// loads observe it) or, inside an ordered sweep, through L2 after the producer's release flag.
 template <class T>
 __device__ __forceinline__ T ldv(const T* p) {
     return *p;
 }
 
-__device__ void ordered_build(const PcgArgs& A, int s) {
-    const DevState& S = A.S;
-    const SceneDev& D = S.scenes[s];
-    const int n = D.n;
-    const long long cb = D.c_begin;
-    auto cid = [&](int i, int j, int k) { return cb + ((long long)i * n + j) * n + k; };
-    auto fluid = [&](int i, int j, int k) {
-        return i >= 0 && j >= 0 && k >= 0 && i < n && j < n && k < n && S.flags[cid(i, j, k)] == ARIEL_FLUID;
-    };
-    if (A.precond == ARIEL_PRECOND_MIC0) {
-        const double tau = A.tau, sigma = A.sigma;
-        hyperplanes(n, false, [&](int i, int j, int k) {
-            long long c = cid(i, j, k);
-            if (S.flags[c] != ARIEL_FLUID) return;
-            double e = A.diag[c];
-            if (fluid(i - 1, j, k)) {
-                double p = ldv(A.pc64 + cid(i - 1, j, k));
-                double ap = -1.0;
-                double oth = (fluid(i - 1, j + 1, k) ? -1.0 : 0.0) + (fluid(i - 1, j, k + 1) ? -1.0 : 0.0);
-                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
-            }
-            if (fluid(i, j - 1, k)) {
-                double p = ldv(A.pc64 + cid(i, j - 1, k));
-                double ap = -1.0;
-                double oth = (fluid(i + 1, j - 1, k) ? -1.0 : 0.0) + (fluid(i, j - 1, k + 1) ? -1.0 : 0.0);
-                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
-            }
-            if (fluid(i, j, k - 1)) {
-                double p = ldv(A.pc64 + cid(i, j, k - 1));
-                double ap = -1.0;
-                double oth = (fluid(i + 1, j, k - 1) ? -1.0 : 0.0) + (fluid(i, j + 1, k - 1) ? -1.0 : 0.0);
-                e -= (ap * p) * (ap * p) + tau * (ap * oth * p * p);
-            }
-            if (e < sigma * A.diag[c]) e = A.diag[c];
-            double pc = e > 0 ? 1.0 / sqrt(e) : 0.0;
-            A.pc64[c] = pc;
-            A.pc32[c] = (float)pc;
-        });
-        return;
-    }
-    if (A.mode == kRef32) {
-        // BuildPreconditioner in serial order, fp32 (solver.inl:104-135)
-        hyperplanes(n, false, [&](int i, int j, int k) {
-            long long c = cid(i, j, k);
-            if (S.flags[c] != ARIEL_FLUID) return;
-            auto term = [&](int a, int b, int cc) {
-                float ar = fluid(a, b, cc) ? -1.0f : 0.0f;  // ARef
-                float pr = 0.0f;                           // PRef: value only if == 1.0f
-                if (a >= 0 && b >= 0 && cc >= 0 && a < n && b < n && cc < n) {
-                    float v = ldv(A.pc32 + cid(a, b, cc));
-                    if (v == 1.0f) pr = v;
-                }
-                return ar * pr;
-            };
-            float left = term(i - 1, j, k), bottom = term(i, j - 1, k), back = term(i, j, k - 1);
-            float diag = (float)A.diag[c];
-            float e = diag - (left * left) - (bottom * bottom) - (back * back);
-            float pc = 0.0f;
-            if (diag > 0) {
-                if (e < 0.25f * diag) e = diag;
-                pc = 1.0f / sqrtf(e);
-            }
-            A.pc32[c] = pc;
-            A.pc64[c] = (double)pc;
-        });
-        return;
-    }
-    hyperplanes(n, false, [&](int i, int j, int k) {
-        long long c = cid(i, j, k);
-        if (S.flags[c] != ARIEL_FLUID) return;
-        auto term = [&](int a, int b, int cc) {
-            return (fluid(a, b, cc) && ldv(A.pc64 + cid(a, b, cc)) == 1.0) ? -1.0 : 0.0;
-        };
-        double left = term(i - 1, j, k), bottom = term(i, j - 1, k), back = term(i, j, k - 1);
-        double dg = A.diag[c];
-        double e = dg - left * left - bottom * bottom - back * back;
-        double pc = 0.0;
-        if (dg > 0) {
-            if (e < 0.25 * dg) e = dg;
-            pc = 1.0 / sqrt(e);
-        }
-        A.pc64[c] = pc;
-        A.pc32[c] = (float)pc;
-    });
+// ------------------------------------------------------------------------------------------
+// Ordered wavefront sweeps over bricks (all blocks of the persistent kernel).
+//
+// The ordered preconditioners (MIC(0), and the reference's PRef == 1 path) need every cell's
+// lower neighbours (i-1, j-1, k-1) before the cell itself (upper ones for the backward
+// sweep).  Each scene's grid is cut into bx*by*bz bricks; a brick depends only on its three
+// upstream bricks, so the bricks of all scenes are listed by level I+J+K and block b takes list
+// positions b, b + G, b + 2G, ...  A brick waits (bounded) for its upstream bricks' progress
+// flags, loads its cells and one face of halo per upstream brick into shared memory, sweeps its
+// own i+j+k levels there, writes the results and publishes its flag.  Every wait points to an
+// earlier list position and every block walks its positions in order, so with all blocks
+// resident (cooperative launch) the sweep always completes.  A cell's arithmetic is the same
+// for any brick shape or grid size.
+// ------------------------------------------------------------------------------------------
+enum BrickKind { kBuild = 0, kFwd = 1, kBwd = 2 };
+
+struct BrickSmem {
+    double* box0;      // [kBrickMaxExt] apply: q (forward) or z (backward) as T; build: pc (double)
+    double* box1;      // [kBrickMaxExt] apply: pc as T
+    double* inb;       // [kBrickMaxCells] interior input: r (forward), q (backward) as T; diag (build)
+    int* lstart;       // [kBrickMaxLevels + 1] first table entry of each level
+    uint16_t* ltab;    // [kBrickMaxCells] packed x << 11 | y << 6 | z, sorted by level x+y+z
+    uint8_t* mbox;     // [kBrickMaxExt] FLUID-neighbour mask | 64 when the cell is FLUID
+};
+
+__device__ BrickSmem brick_smem(unsigned char* dyn) {
+    BrickSmem B;
+    B.box0 = reinterpret_cast<double*>(dyn);
+    B.box1 = B.box0 + kBrickMaxExt;
+    B.inb = B.box1 + kBrickMaxExt;
+    B.lstart = reinterpret_cast<int*>(B.inb + kBrickMaxCells);
+    B.ltab = reinterpret_cast<uint16_t*>(B.lstart + kBrickMaxLevels + 1);
+    B.mbox = reinterpret_cast<uint8_t*>(B.ltab + kBrickMaxCells);
+    return B;
 }
 
-// z = M^-1 r by ordered forward and backward sweeps over one scene (T = vector type).
-template <class T>
-__device__ void ordered_apply(const PcgArgs& A, int s, const T* r, T* z, T* q, const T* pc, bool ref32) {
+// The brick's cells grouped by level (built once per launch).
+__device__ void brick_levels(const PcgArgs& A, BrickSmem& B) {
+    const int bx = A.bx, by = A.by, bz = A.bz, nl = bx + by + bz - 2, ncell = bx * by * bz;
+    int* cur = reinterpret_cast<int*>(B.box0);
+    for (int l = threadIdx.x; l <= nl; l += blockDim.x) B.lstart[l] = 0;
+    __syncthreads();
+    for (int li = threadIdx.x; li < ncell; li += blockDim.x) {
+        const int x = li / (by * bz), y = (li / bz) % by, z = li % bz;
+        atomicAdd(&B.lstart[x + y + z + 1], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int l = 1; l <= nl; ++l) B.lstart[l] += B.lstart[l - 1];
+    __syncthreads();
+    for (int l = threadIdx.x; l < nl; l += blockDim.x) cur[l] = B.lstart[l];
+    __syncthreads();
+    for (int li = threadIdx.x; li < ncell; li += blockDim.x) {
+        const int x = li / (by * bz), y = (li / bz) % by, z = li % bz;
+        const int pos = atomicAdd(&cur[x + y + z], 1);
+        B.ltab[pos] = (uint16_t)((x << 11) | (y << 6) | z);
+    }
+    __syncthreads();
+}
+
+// Thread 0: bounded wait until *f >= val.
+__device__ bool brick_wait(const unsigned* f, unsigned val, Barrier* bar, int* dev_error, unsigned long long tmo) {
+    const unsigned long long t0 = gtimer();
+    while (ld_acquire_u32(f) < val) {
+        if (*(volatile int*)&bar->error) return false;
+        if (gtimer() - t0 > tmo) {
+            atomicExch(&bar->error, 1);
+            if (dev_error) atomicExch(dev_error, 1);
+            return false;
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
+// One sweep over the bricks of every ordered scene (apply sweeps skip scenes whose inner solve
+// is done).  KIND kBuild: the preconditioner values (pc64 / pc32); kFwd: out = q from in = r;
+// kBwd: out = z from in = q.  `val` is this sweep's flag value (the forward sweep's is val - 1
+// for kBwd).  Returns false when a wait gave up.
+template <int KIND, class T>
+__device__ bool brick_sweep(const PcgArgs& A, const BrickSmem& B, unsigned val, const T* in, T* out, const T* pcv,
+                            unsigned long long tmo) {
     const DevState& S = A.S;
-    const SceneDev& D = S.scenes[s];
-    const int n = D.n;
-    const long long cb = D.c_begin;
     const bool mic = A.precond == ARIEL_PRECOND_MIC0;
-    auto cid = [&](int i, int j, int k) { return cb + ((long long)i * n + j) * n + k; };
-    auto fluid = [&](int i, int j, int k) {
-        return i >= 0 && j >= 0 && k >= 0 && i < n && j < n && k < n && S.flags[cid(i, j, k)] == ARIEL_FLUID;
-    };
-    hyperplanes(n, false, [&](int i, int j, int k) {
-        long long c = cid(i, j, k);
-        if (S.flags[c] != ARIEL_FLUID) return;
-        const int lo[3][3] = {{i - 1, j, k}, {i, j - 1, k}, {i, j, k - 1}};
-        T t = ldv(r + c);
-        for (int m = 0; m < 3; ++m) {
-            if (!fluid(lo[m][0], lo[m][1], lo[m][2])) continue;
-            long long qc = cid(lo[m][0], lo[m][1], lo[m][2]);
-            T pq = ldv(pc + qc), qq = ldv(q + qc);
-            if (mic)
-                t -= (T)-1.0 * pq * qq;
-            else if (pq == (T)1.0 && qq == (T)1.0)
-                t -= (T)-1.0;  // ARef*PRef(P)*PRef(Q) = -1
+    const bool ref32 = A.mode == kRef32;
+    const int bx = A.bx, by = A.by, bz = A.bz;
+    const int ey = by + 1, ez = bz + 1;
+    const int sx = ey * ez, sy = ez;
+    const int lo = KIND == kBwd ? 0 : 1;  // halo below (build, forward) or above (backward)
+    const int nl = bx + by + bz - 2, ncell = bx * by * bz;
+    const int nb = A.nbricks;
+    T* const vbox = reinterpret_cast<T*>(B.box0);
+    T* const pbox = reinterpret_cast<T*>(B.box1);
+    double* const cbox = B.box0;
+    T* const vin = reinterpret_cast<T*>(B.inb);
+    double* const din = B.inb;
+    const int nfx = by * bz, nfy = bx * bz, nfz = bx * by, nh = nfx + nfy + nfz;
+    const int hx = KIND == kBwd ? bx : -1, hy = KIND == kBwd ? by : -1, hz = KIND == kBwd ? bz : -1;
+    auto bidx = [&](int x, int y, int z) { return ((x + lo) * ey + (y + lo)) * ez + (z + lo); };
+    __shared__ int s_ok;
+    for (int p = blockIdx.x; p < nb; p += gridDim.x) {
+        const int pp = KIND == kBwd ? nb - 1 - p : p;
+        const int4 br = A.bricks[pp];
+        const int s = br.x;
+        if (!ldv(&A.sc[s].ordered)) continue;
+        if (KIND != kBuild && ldv(&A.sc[s].inner_done)) continue;
+        const SceneDev& D = S.scenes[s];
+        const int n = D.n;
+        const int I0 = br.y * bx, J0 = br.z * by, K0 = br.w * bz;
+        const int nbJ = (n + by - 1) / by, nbK = (n + bz - 1) / bz, nbI = (n + bx - 1) / bx;
+        unsigned* const fb = A.bflag + A.brick_base[s];
+        auto flag_of = [&](int I, int J, int K) { return fb + ((long long)I * nbJ + J) * nbK + K; };
+        auto inside = [&](int i, int j, int k) { return i >= 0 && j >= 0 && k >= 0 && i < n && j < n && k < n; };
+        auto cid = [&](int i, int j, int k) { return D.c_begin + ((long long)i * n + j) * n + k; };
+        auto halo_cell = [&](int h, int& x, int& y, int& z) -> bool {
+            if (h < nfx) {
+                x = hx;
+                y = h / bz;
+                z = h % bz;
+            } else if (h < nfx + nfy) {
+                h -= nfx;
+                x = h / bz;
+                y = hy;
+                z = h % bz;
+            } else {
+                h -= nfx + nfy;
+                x = h / by;
+                y = h % by;
+                z = hz;
+            }
+            return inside(I0 + x, J0 + y, K0 + z);
+        };
+        // 1. data that does not change during the sweep: masks, r (forward), pc, diagonal
+        for (int li = threadIdx.x; li < ncell; li += blockDim.x) {
+            const int x = li / (by * bz), y = (li / bz) % by, z = li % bz;
+            const int bi = bidx(x, y, z);
+            uint8_t m = 0;
+            if (inside(I0 + x, J0 + y, K0 + z)) {
+                const long long c = cid(I0 + x, J0 + y, K0 + z);
+                if (S.flags[c] == ARIEL_FLUID) {
+                    m = (uint8_t)(A.mask[c] | 64);
+                    if (KIND == kBuild) {
+                        din[li] = A.diag[c];
+                    } else {
+                        pbox[bi] = pcv[c];
+                        if (KIND == kFwd) vin[li] = in[c];
+                    }
+                }
+            }
+            B.mbox[bi] = m;
         }
-        q[c] = t * ldv(pc + c);
-    });
-    hyperplanes(n, true, [&](int i, int j, int k) {
-        long long c = cid(i, j, k);
-        if (S.flags[c] != ARIEL_FLUID) return;
-        const int hi[3][3] = {{i + 1, j, k}, {i, j + 1, k}, {i, j, k + 1}};
-        T pcc = ldv(pc + c);
-        T t = ldv(q + c);
-        for (int m = 0; m < 3; ++m) {
-            if (!fluid(hi[m][0], hi[m][1], hi[m][2])) continue;
-            long long qc = cid(hi[m][0], hi[m][1], hi[m][2]);
-            T zq = ldv(z + qc);
-            if (mic)
-                t -= (T)-1.0 * pcc * zq;
-            else if (pcc == (T)1.0 && zq == (T)1.0)
-                t -= (T)-1.0;
+        for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+            int x, y, z;
+            const bool ok = halo_cell(h, x, y, z);
+            const int bi = bidx(x, y, z);
+            uint8_t m = 0;
+            if (ok) {
+                const long long c = cid(I0 + x, J0 + y, K0 + z);
+                if (S.flags[c] == ARIEL_FLUID) {
+                    m = (uint8_t)(A.mask[c] | 64);
+                    if (KIND == kFwd) pbox[bi] = pcv[c];
+                }
+            }
+            B.mbox[bi] = m;
         }
-        z[c] = t * pcc;
-    });
-    (void)ref32;
+        // 2. upstream bricks (and, backward, this brick's forward sweep)
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            if (KIND == kBwd) {
+                ok = brick_wait(flag_of(br.y, br.z, br.w), val - 1, A.bar, S.dev_error, tmo);
+                if (ok && br.y + 1 < nbI) ok = brick_wait(flag_of(br.y + 1, br.z, br.w), val, A.bar, S.dev_error, tmo);
+                if (ok && br.z + 1 < nbJ) ok = brick_wait(flag_of(br.y, br.z + 1, br.w), val, A.bar, S.dev_error, tmo);
+                if (ok && br.w + 1 < nbK) ok = brick_wait(flag_of(br.y, br.z, br.w + 1), val, A.bar, S.dev_error, tmo);
+            } else {
+                if (br.y > 0) ok = brick_wait(flag_of(br.y - 1, br.z, br.w), val, A.bar, S.dev_error, tmo);
+                if (ok && br.z > 0) ok = brick_wait(flag_of(br.y, br.z - 1, br.w), val, A.bar, S.dev_error, tmo);
+                if (ok && br.w > 0) ok = brick_wait(flag_of(br.y, br.z, br.w - 1), val, A.bar, S.dev_error, tmo);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) return false;
+        // 3. what the upstream bricks produced, read through L2
+        if (KIND == kBwd)
+            for (int li = threadIdx.x; li < ncell; li += blockDim.x) {
+                const int x = li / (by * bz), y = (li / bz) % by, z = li % bz;
+                if (B.mbox[bidx(x, y, z)] & 64) vin[li] = __ldcg(in + cid(I0 + x, J0 + y, K0 + z));
+            }
+        for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+            int x, y, z;
+            if (!halo_cell(h, x, y, z)) continue;
+            const int bi = bidx(x, y, z);
+            if (!(B.mbox[bi] & 64)) continue;
+            const long long c = cid(I0 + x, J0 + y, K0 + z);
+            if (KIND == kBuild)
+                cbox[bi] = ref32 ? (double)__ldcg(A.pc32 + c) : __ldcg(A.pc64 + c);
+            else
+                vbox[bi] = __ldcg(out + c);
+        }
+        __syncthreads();
+        // 4. the brick's own levels (highest first for the backward sweep)
+        for (int lv = 0; lv < nl; ++lv) {
+            const int l = KIND == kBwd ? nl - 1 - lv : lv;
+            for (int e = B.lstart[l] + threadIdx.x; e < B.lstart[l + 1]; e += blockDim.x) {
+                const unsigned pk = B.ltab[e];
+                const int x = (int)(pk >> 11), y = (int)((pk >> 6) & 31u), z = (int)(pk & 63u);
+                const int bi = bidx(x, y, z);
+                const unsigned m = B.mbox[bi];
+                if (!(m & 64u)) continue;
+                const int li = (x * by + y) * bz + z;
+                if (KIND == kFwd) {
+                    // q = (r - sum_lower a pc_q q_q) pc
+                    T t = vin[li];
+                    const int offs[3] = {-sx, -sy, -1};
+                    const unsigned bits[3] = {1u, 4u, 16u};
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (!(m & bits[d])) continue;
+                        const T pq = pbox[bi + offs[d]], qq = vbox[bi + offs[d]];
+                        if (mic)
+                            t -= (T)-1.0 * pq * qq;
+                        else if (pq == (T)1.0 && qq == (T)1.0)
+                            t -= (T)-1.0;  // ARef*PRef(P)*PRef(Q) = -1
+                    }
+                    vbox[bi] = t * pbox[bi];
+                } else if (KIND == kBwd) {
+                    // z = (q - sum_upper a pc z_q) pc
+                    const T pcc = pbox[bi];
+                    T t = vin[li];
+                    const int offs[3] = {sx, sy, 1};
+                    const unsigned bits[3] = {2u, 8u, 32u};
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (!(m & bits[d])) continue;
+                        const T zq = vbox[bi + offs[d]];
+                        if (mic)
+                            t -= (T)-1.0 * pcc * zq;
+                        else if (pcc == (T)1.0 && zq == (T)1.0)
+                            t -= (T)-1.0;
+                    }
+                    vbox[bi] = t * pcc;
+                } else if (mic) {
+                    // MIC(0) (Bridson): e = diag - sum_lower [(a p)^2 + tau a (sum of the lower
+                    // neighbour's other upper couplings) p^2], safety sigma
+                    const double tau = A.tau, sigma = A.sigma, ap = -1.0;
+                    const double dg = din[li];
+                    double e = dg;
+                    const int offs[3] = {-sx, -sy, -1};
+                    const unsigned bits[3] = {1u, 4u, 16u};
+                    const unsigned oa[3] = {8u, 2u, 2u}, ob[3] = {32u, 32u, 8u};
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        if (!(m & bits[d])) continue;
+                        const double pq = cbox[bi + offs[d]];
+                        const unsigned mq = B.mbox[bi + offs[d]];
+                        const double oth = ((mq & oa[d]) ? -1.0 : 0.0) + ((mq & ob[d]) ? -1.0 : 0.0);
+                        e -= (ap * pq) * (ap * pq) + tau * (ap * oth * pq * pq);
+                    }
+                    if (e < sigma * dg) e = dg;
+                    cbox[bi] = e > 0 ? 1.0 / sqrt(e) : 0.0;
+                } else if (ref32) {
+                    // BuildPreconditioner in fp32 (solver.inl:104-135)
+                    auto term = [&](unsigned bit, int off) -> float {
+                        return ((m & bit) && (float)cbox[bi + off] == 1.0f) ? -1.0f : 0.0f;
+                    };
+                    const float left = term(1u, -sx), bottom = term(4u, -sy), back = term(16u, -1);
+                    const float diag = (float)din[li];
+                    float e = diag - (left * left) - (bottom * bottom) - (back * back);
+                    float pc = 0.0f;
+                    if (diag > 0) {
+                        if (e < 0.25f * diag) e = diag;
+                        pc = 1.0f / sqrtf(e);
+                    }
+                    cbox[bi] = (double)pc;
+                } else {
+                    auto term = [&](unsigned bit, int off) -> double {
+                        return ((m & bit) && cbox[bi + off] == 1.0) ? -1.0 : 0.0;
+                    };
+                    const double left = term(1u, -sx), bottom = term(4u, -sy), back = term(16u, -1);
+                    const double dg = din[li];
+                    double e = dg - left * left - bottom * bottom - back * back;
+                    double pc = 0.0;
+                    if (dg > 0) {
+                        if (e < 0.25 * dg) e = dg;
+                        pc = 1.0 / sqrt(e);
+                    }
+                    cbox[bi] = pc;
+                }
+            }
+            __syncthreads();
+        }
+        // 5. results out, then publish the brick
+        for (int li = threadIdx.x; li < ncell; li += blockDim.x) {
+            const int x = li / (by * bz), y = (li / bz) % by, z = li % bz;
+            const int bi = bidx(x, y, z);
+            if (!(B.mbox[bi] & 64)) continue;
+            const long long c = cid(I0 + x, J0 + y, K0 + z);
+            if (KIND == kBuild) {
+                const double pc = cbox[bi];
+                A.pc64[c] = pc;
+                A.pc32[c] = (float)pc;
+            } else {
+                out[c] = vbox[bi];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_u32(flag_of(br.y, br.z, br.w), val);
+        }
+    }
+    return true;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -548,10 +707,13 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
     // elementwise preconditioner of the reference ((r*pc)*pc) for non-ordered scenes
     auto precond_elem = [&](long long c, T rv) -> T { return (rv * ldv(pcv + c)) * ldv(pcv + c); };
 
-    // ---- Phase 0: ordered preconditioner build -------------------------------------------
+    // ---- Phase 0: ordered preconditioner build (brick wavefront) ---------------------------
+    extern __shared__ __align__(16) unsigned char kdyn[];
+    BrickSmem BS = brick_smem(kdyn);
+    unsigned bseq = 0;  // progress-flag value of the latest sweep (same in every block)
     if (any_ordered) {
-        for (int s = blockIdx.x; s < k; s += gridDim.x)
-            if (ldv(&SC[s].ordered)) ordered_build(A, s);
+        brick_levels(A, BS);
+        if (!brick_sweep<kBuild, double>(A, BS, ++bseq, nullptr, nullptr, nullptr, tmo)) return;
         if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
     }
 
@@ -844,24 +1006,29 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
             if (!ord) write_part(ch, a0, 0.0);
         }
         if (any_ordered) {
+            // z = M^-1 r for the ordered scenes: forward then backward brick sweeps, then z.r
+            // per chunk like every other scene
             if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
-            for (int s = blockIdx.x; s < k; s += gridDim.x) {
-                if (!ldv(&SC[s].ordered) || ldv(&SC[s].inner_done)) continue;
-                ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
+            ++bseq;
+            if (!brick_sweep<kFwd, T>(A, BS, bseq, r, ordq, pcv, tmo)) return;
+            ++bseq;
+            if (!brick_sweep<kBwd, T>(A, BS, bseq, ordq, z, pcv, tmo)) return;
+            if (!grid_barrier(A.bar, S.dev_error, tmo, NoLeader{})) return;
+            for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                int s;
+                long long t0, t1;
+                chunk_range(ch, s, t0, t1);
+                if (!ldv(&SC[s].ordered)) continue;
                 double a0 = 0.0;
-                for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
-                    long long c = A.fl[t];
-                    T zv = ldv(z + c);
-                    sb0[c] = zv;
-                    a0 += (double)zv * (double)ldv(r + c);
-                }
-                double b0 = 0.0;
-                block_sum2(a0, b0);
-                if (threadIdx.x == 0)
-                    for (long long ch = ch_s[s]; ch < ch_s[s + 1]; ++ch) {
-                        part0[ch] = ch == ch_s[s] ? a0 : 0.0;
-                        part1[ch] = 0.0;
+                if (!ldv(&SC[s].inner_done)) {
+                    for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                        long long c = A.fl[t];
+                        T zv = ldv(z + c);
+                        sb0[c] = zv;
+                        a0 += (double)zv * (double)ldv(r + c);
                     }
+                }
+                write_part(ch, a0, 0.0);
             }
         }
         ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
@@ -979,18 +1146,26 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
                     block_sum2(a1, b0);
                     if (threadIdx.x == 0) part1[ch] = a1;
                 }
-                for (int s = blockIdx.x; s < k; s += gridDim.x) {
-                    if (!ldv(&SC[s].ordered) || ldv(&SC[s].inner_done)) continue;
-                    ordered_apply<T>(A, s, r, z, ordq, pcv, MODE == kRef32);
+                ++bseq;
+                if (!brick_sweep<kFwd, T>(A, BS, bseq, r, ordq, pcv, tmo)) return;
+                ++bseq;
+                if (!brick_sweep<kBwd, T>(A, BS, bseq, ordq, z, pcv, tmo)) return;
+                ok = grid_barrier(A.bar, S.dev_error, tmo, NoLeader{});
+                if (!ok) return;
+                for (long long ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+                    int s;
+                    long long t0, t1;
+                    chunk_range(ch, s, t0, t1);
+                    if (!ldv(&SC[s].ordered)) continue;
                     double a1 = 0.0;
-                    for (long long t = fl_s[s] + threadIdx.x; t < fl_s[s + 1]; t += blockDim.x) {
-                        long long c = A.fl[t];
-                        a1 += (double)ldv(z + c) * (double)ldv(r + c);
-                    }
+                    if (!ldv(&SC[s].inner_done))
+                        for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+                            long long c = A.fl[t];
+                            a1 += (double)ldv(z + c) * (double)ldv(r + c);
+                        }
                     double b0 = 0.0;
                     block_sum2(a1, b0);
-                    if (threadIdx.x == 0)
-                        for (long long ch = ch_s[s]; ch < ch_s[s + 1]; ++ch) part1[ch] = ch == ch_s[s] ? a1 : 0.0;
+                    if (threadIdx.x == 0) part1[ch] = a1;
                 }
             }
             ok = grid_barrier(A.bar, S.dev_error, tmo, [&]() {
@@ -1102,6 +1277,7 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
     cudaMemsetAsync(A.sc, 0, sizeof(PcgScene) * (size_t)S.k, st);
     cudaMemsetAsync(A.ctl, 0, sizeof(PcgCtl), st);
     cudaMemsetAsync(A.bar, 0, sizeof(Barrier), st);
+    if (A.nbricks > 0) cudaMemsetAsync(A.bflag, 0, sizeof(unsigned) * (size_t)A.nbricks, st);
     if (S.nc > 0) {
         k_prep_cells<<<grid_for(S.nc), kBlock, 0, st>>>(A, pred);
         count_launch();
@@ -1792,7 +1968,7 @@ static cudaError_t coop_launch(const PcgArgs& A, int nblocks, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)nblocks);
     cfg.blockDim = dim3(kPcgThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = brick_dyn_smem();
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
@@ -1848,17 +2024,21 @@ int pcg_max_blocks(int device, int mode, int per_sm_cap) {
     cudaError_t e;
     int per_fast = 0;
     const int dyn = (int)fast_dyn_smem(mode);
+    const int bdyn = (int)brick_dyn_smem();
     if (mode == kRef32) {
         cudaFuncSetAttribute(k_pcg_fast<kRef32>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kRef32>, kPcgThreads, 0);
+        cudaFuncSetAttribute(k_pcg<kRef32>, cudaFuncAttributeMaxDynamicSharedMemorySize, bdyn);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kRef32>, kPcgThreads, bdyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kRef32>, kPcgThreads, dyn);
     } else if (mode == kFp64) {
         cudaFuncSetAttribute(k_pcg_fast<kFp64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kFp64>, kPcgThreads, 0);
+        cudaFuncSetAttribute(k_pcg<kFp64>, cudaFuncAttributeMaxDynamicSharedMemorySize, bdyn);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kFp64>, kPcgThreads, bdyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kFp64>, kPcgThreads, dyn);
     } else {
         cudaFuncSetAttribute(k_pcg_fast<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kMixed>, kPcgThreads, 0);
+        cudaFuncSetAttribute(k_pcg<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, bdyn);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<kMixed>, kPcgThreads, bdyn);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_fast, k_pcg_fast<kMixed>, kPcgThreads, dyn);
     }
     if (per_fast < per) per = per_fast;  // one grid size serves both kernels
@@ -1874,6 +2054,16 @@ cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long t
     k_barrier_selftest<<<2, 32, 0, st>>>(bar, err, timeout_ns);
     count_launch();
     return cudaGetLastError();
+}
+
+size_t brick_dyn_smem() {
+    return (size_t)2 * kBrickMaxExt * 8 + (size_t)kBrickMaxCells * 8 + (size_t)(kBrickMaxLevels + 1) * 4 +
+           (size_t)kBrickMaxCells * 2 + (size_t)kBrickMaxExt;
+}
+
+bool brick_shape_ok(int bx, int by, int bz) {
+    return bx >= 1 && by >= 1 && bz >= 1 && bx <= 31 && by <= 31 && bz <= 63 && bx * by * bz <= kBrickMaxCells &&
+           (bx + 1) * (by + 1) * (bz + 1) <= kBrickMaxExt && bx + by + bz - 2 <= kBrickMaxLevels;
 }
 
 }  // namespace ariel

@@ -89,6 +89,13 @@ struct PcgArgs {
     float* d32;      // MIXED inner correction
     double* partial; // 3 * max chunks (three dot products per reduction)
     long long max_chunks;
+    // ordered wavefront sweeps: bricks of every scene sorted by level I+J+K (then scene, I, J,
+    // K), each scene's brick grid starting at brick_base[s], one progress flag per brick
+    const int4* bricks;
+    const int* brick_base;
+    unsigned* bflag;
+    int nbricks;
+    int bx, by, bz;
     PcgScene* sc;
     PcgTotals* totals;
     PcgCtl* ctl;
@@ -105,5 +112,11 @@ int pcg_max_blocks(int device, int mode, int per_sm_cap);
 cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long timeout_ns, cudaStream_t st);
 
 constexpr int kPcgThreads = 256;
+constexpr int kBrickMaxCells = 2048;
+constexpr int kBrickMaxExt = 2744;
+constexpr int kBrickMaxLevels = 128;
+// Dynamic shared memory of the general solve kernel (the ordered wavefront sweeps' boxes).
+size_t brick_dyn_smem();
+bool brick_shape_ok(int bx, int by, int bz);
 
 }  // namespace ariel

@@ -124,10 +124,13 @@ def load_traffic(workload):
         return None
 
 
+PRECOND = "ref"
+
+
 def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
     p = A.params_default()
     p.precision = precision
-    p.precond = A.PRECOND_REF
+    p.precond = A.PRECOND_MIC0 if PRECOND == "mic0" else A.PRECOND_REF
     p.stop_rule = A.STOP_REL
     p.tol = tol
     p.use_graph = graph
@@ -272,7 +275,8 @@ def config_dict(args, n_particles, ws):
     return {"workload": "dam break %d^3, %d particles per scene, mixed-precision PCG to %g relative residual"
             % (args.n, n_particles, args.tol),
             "grid": args.n, "particles_per_scene": n_particles, "scenes": ws, "precision": args.precision,
-            "preconditioner": "reference (solver.inl:104-135)", "tolerance": args.tol, "dt": 1.0 / 240.0,
+            "preconditioner": ("MIC(0), tau 0.97" if args.precond == "mic0" else "reference (solver.inl:104-135)"),
+            "tolerance": args.tol, "dt": 1.0 / 240.0,
             "parallelism": "replicas" if ws > 1 else "single",
             "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
 
@@ -366,7 +370,11 @@ def main():
     ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--max-live", type=int, default=32)
+    ap.add_argument("--precond", choices=["ref", "mic0"], default="ref",
+                    help="ref: the reference's preconditioner (solver.inl:104-135); mic0: MIC(0), tau .97")
     args = ap.parse_args()
+    global PRECOND
+    PRECOND = args.precond
     if args.workload == "sphere" and args.n == 128:
         args.n = 256
     if args.warmup < 3 and args.impl == "ours":

@@ -159,6 +159,10 @@ typedef struct AsimParams {
     int32_t pcg_blocks_per_sm;  /* blocks per SM of the persistent solve kernel; 0 = default (2) */
     int32_t pcg_grid_blocks;    /* >0: cap on the solve kernel's blocks in all (results do not
                                    depend on it; tests and tuning); 0 = one grid of resident blocks */
+    int32_t sweep_brick[3];     /* brick (i, j, k extents in cells) of the ordered wavefront sweeps
+                                   (MIC(0) and the reference's PRef==1 path); results do not depend
+                                   on it.  0,0,0 = default 8,16,16.  Limits: i,j <= 31, k <= 63,
+                                   product <= 2048, (i+1)(j+1)(k+1) <= 2744 */
 } AsimParams;
 
 typedef struct AsimStats {

@@ -98,13 +98,15 @@ def _pocket_grids(n=8):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [A.PREC_REF32, A.PREC_FP64])
-def test_pref_quirk_ordered_path(precision):
+@pytest.mark.parametrize("precision,brick", [(A.PREC_REF32, (0, 0, 0)), (A.PREC_FP64, (0, 0, 0)),
+                                             (A.PREC_REF32, (2, 2, 2)), (A.PREC_FP64, (3, 2, 4))])
+def test_pref_quirk_ordered_path(precision, brick):
     n = 8
     g = _pocket_grids(n)
     desc = dambreak(n)
     # a fixed, small iteration count makes the pressure depend on the preconditioner itself
     prm = params(precision=precision, stop=A.STOP_REL, tol=1e-14, max_iters=3)
+    prm.sweep_brick[:] = brick
     ora = RefSim(desc, prm)
     st = dict(pos=np.array([[0.1, 0.1, 0.1]], np.float32), vel=np.zeros((1, 3), np.float32),
               mass=np.ones(1, np.float32), type=np.array([A.FLUID], np.int32))
@@ -123,12 +125,13 @@ def test_pref_quirk_ordered_path(precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
-def test_mic0_against_oracle(precision):
-    n = 16
+@pytest.mark.parametrize("precision,n,brick", [(A.PREC_FP64, 16, (0, 0, 0)), (A.PREC_MIXED, 16, (0, 0, 0)),
+                                               (A.PREC_FP64, 24, (4, 4, 8)), (A.PREC_MIXED, 24, (5, 3, 7))])
+def test_mic0_against_oracle(precision, n, brick):
     desc, st, g = _solve_inputs(n, seed=9, steps=5)
     # MIC(0) after three iterations (FP64 oracle, serial lexicographic factorisation)
     prm = params(precision=A.PREC_FP64, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-14, max_iters=3)
+    prm.sweep_brick[:] = brick
     ora = RefSim(desc, prm)
     ora.set_particles(st["pos"], st["vel"], st["mass"], st["type"])
     for w, key in [(A.GRID_A, "A"), (A.GRID_L, "L"), (A.GRID_D, "D"), (A.GRID_P, "P"), (A.GRID_P64, "P64")]:
@@ -143,7 +146,9 @@ def test_mic0_against_oracle(precision):
     # converged MIC(0) solves reach the FP64 oracle's solution and need fewer iterations than
     # the reference's diagonal preconditioner
     xstar, _, _ = solve_fp64(n, g["A"], g["L"], g["D"].astype(np.float64).ravel(), tol=1e-12)
-    mic = _gpu_solve(desc, st, g, params(precision=precision, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-7))
+    pm = params(precision=precision, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-7)
+    pm.sweep_brick[:] = brick
+    mic = _gpu_solve(desc, st, g, pm)
     ref = _gpu_solve(desc, st, g, params(precision=precision, precond=A.PRECOND_REF, stop=A.STOP_REL, tol=1e-7))
     assert mic["stats"].pcg_converged
     err = np.linalg.norm((mic["P64"] - xstar)[fl]) / np.linalg.norm(xstar[fl])
@@ -165,3 +170,33 @@ def test_solve_independent_of_grid_size(precision):
         assert np.array_equal(runs[0][key].view(np.uint8), runs[1][key].view(np.uint8)), key
     assert runs[0]["stats"].pcg_iterations == runs[1]["stats"].pcg_iterations
     assert runs[0]["stats"].pcg_converged == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_mic0_independent_of_brick_and_grid(precision):
+    """The wavefront sweeps give the same bits for any brick shape and any number of blocks:
+    each cell's update reads the same values in the same order, only the schedule changes."""
+    desc, st, g = _solve_inputs(32, seed=9, steps=5)
+    runs = []
+    for brick, nb in [((0, 0, 0), 0), ((4, 4, 8), 0), ((8, 8, 32), 0), ((16, 16, 8), 0), ((3, 5, 7), 1)]:
+        prm = params(precision=precision, precond=A.PRECOND_MIC0, stop=A.STOP_REL, tol=1e-7, pcg_grid_blocks=nb)
+        prm.sweep_brick[:] = brick
+        runs.append(_gpu_solve(desc, st, g, prm))
+    for r in runs[1:]:
+        assert np.array_equal(r["P64"].view(np.uint8), runs[0]["P64"].view(np.uint8))
+        assert r["stats"].pcg_iterations == runs[0]["stats"].pcg_iterations
+    assert runs[0]["stats"].pcg_converged == 1
+
+
+def test_sweep_brick_limits_checked():
+    """Brick shapes outside the shared-memory layout are refused before any device work."""
+    import ctypes as C
+    from ariel_b200 import _lib
+    L = _lib.lib()
+    d = A.scene_dambreak(16)
+    for bad in [(32, 1, 1), (1, 1, 64), (16, 16, 16), (0, 4, 4), (-1, 4, 4)]:
+        p = A.params_default()
+        p.sweep_brick[:] = bad
+        h = C.c_void_p()
+        assert L.ariel_create(C.byref(d), C.byref(p), C.byref(h)) == A.ARIEL_ERR_INVALID_ARG
