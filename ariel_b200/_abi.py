@@ -98,7 +98,8 @@ REQ_QUEUED, REQ_READY, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(5)
 class AsimServerConfig(C.Structure):
     _fields_ = [
         ("hbm_budget_bytes", C.c_int64), ("max_live", C.c_int32), ("prepare_threads", C.c_int32),
-        ("keep_results", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("keep_results", C.c_int32), ("max_ready", C.c_int32), ("reserve_budget", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -122,6 +123,8 @@ class AsimServerStats(C.Structure):
         ("relayouts", C.c_int64), ("relayout_ms", C.c_double),
         ("hbm_budget_bytes", C.c_int64), ("hbm_in_use_bytes", C.c_int64), ("hbm_peak_bytes", C.c_int64),
         ("max_live_seen", C.c_int32), ("last_error", C.c_int32),
+        ("relayout_wait_ms", C.c_double), ("relayout_build_ms", C.c_double), ("graph_build_ms", C.c_double),
+        ("staged", C.c_int64),
     ]
 
 

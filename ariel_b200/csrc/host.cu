@@ -443,12 +443,13 @@ long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector
 void free_scratch(ariel_sim* s) { free_bufs(s, true); }
 
 ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ariel_sim* src,
-                         const std::vector<int>* src_idx) {
+                         const std::vector<int>* src_idx, const std::vector<DeviceParticles>* staged) {
     free_all(s);
     const int k = s->k;
     auto from_src = [&](int i) { return src && src_idx && (*src_idx)[i] >= 0; };
+    auto from_staged = [&](int i) { return !from_src(i) && staged && (*staged)[i].valid; };
     for (int i = 0; i < k; ++i)
-        if (!from_src(i) && !hp[i].binned) bin_solids(s->descs[i], hp[i]);
+        if (!from_src(i) && !from_staged(i) && !hp[i].binned) bin_solids(s->descs[i], hp[i]);
     s->ppref.assign(k + 1, 0);
     s->cpref.assign(k + 1, 0);
     s->fpref.assign(k + 1, 0);
@@ -462,6 +463,9 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
             const int j = (*src_idx)[i];
             cnt = src->ppref[j + 1] - src->ppref[j];
             scnt = src->spref[j + 1] - src->spref[j];
+        } else if (from_staged(i)) {
+            cnt = (*staged)[i].np;
+            scnt = (*staged)[i].ns;
         } else {
             cnt = (long long)hp[i].pos4.size();
             scnt = (long long)hp[i].solid_pos.size();
@@ -660,6 +664,22 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
             }
             ARIEL_CUDA(cudaMemcpyAsync(A.sc + i, src->PA.sc + j, sizeof(PcgScene), cudaMemcpyDeviceToDevice, st));
             ARIEL_CUDA(cudaMemcpyAsync(A.totals + i, src->PA.totals + j, sizeof(PcgTotals), cudaMemcpyDeviceToDevice, st));
+            continue;
+        }
+        if (from_staged(i)) {
+            // a new scene already uploaded: device copies only
+            const DeviceParticles& g = (*staged)[i];
+            if (cnt > 0) {
+                ARIEL_CUDA(cudaMemcpyAsync(S.pos4 + pb, g.pos4, cnt * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+                ARIEL_CUDA(cudaMemcpyAsync(S.vel4 + pb, g.vel4, cnt * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+            }
+            if (scnt > 0) {
+                ARIEL_CUDA(cudaMemcpyAsync(S.solid_pos + sb, g.solid_pos, scnt * sizeof(float4),
+                                           cudaMemcpyDeviceToDevice, st));
+                ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, g.solid_start, ncell, (uint32_t)sb, st));
+            } else {
+                ARIEL_CUDA(launch_u32_offset(S.solid_start + cb, nullptr, ncell, (uint32_t)sb, st));
+            }
             continue;
         }
         if (cnt > 0) {

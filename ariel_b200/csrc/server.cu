@@ -37,6 +37,8 @@ struct Request {
     ariel_status status = ARIEL_OK;
     int32_t steps_done = 0;  // steps queued on the device
     HostParticles hp;
+    DeviceParticles dev;       // the same particles uploaded ahead of admission, when they fit
+    long long staged_bytes = 0;
     long long np = 0, ns = 0, bytes = 0;
     double t_submit = -1, t_admit = -1, t_done = -1;
     std::vector<float> pos, vel;
@@ -71,6 +73,8 @@ struct ariel_server {
     int64_t next_id = 1;
     std::map<int64_t, std::unique_ptr<Request>> reqs;
     std::deque<Request*> to_prepare;
+    int preparing = 0;                  // being seeded by a host thread
+    long long staged_total = 0;         // device bytes of uploaded, not yet admitted scenes
     std::map<int64_t, Request*> ready;  // prepared, waiting for device memory, oldest first
     std::vector<Request*> live;         // batch order
     ariel_sim* batch = nullptr;         // worker thread only
@@ -80,7 +84,8 @@ struct ariel_server {
     std::vector<double> latency_ms;
     int64_t batch_steps = 0, particle_steps = 0, submitted = 0, admitted = 0, finished = 0, failed = 0;
     int64_t relayouts = 0;
-    double relayout_ms = 0, busy_ms = 0;
+    double relayout_ms = 0, busy_ms = 0, relayout_wait_ms = 0, relayout_build_ms = 0, graph_build_ms = 0;
+    int64_t staged = 0;
     long long in_use = 0, peak = 0;
     int max_live_seen = 0;
     ariel_status last_error = ARIEL_OK;
@@ -102,15 +107,81 @@ long long bufs_bytes(const ariel_sim* s, bool keep_only) {
     return b;
 }
 
+void free_staged(ariel_server* S, Request* r, cudaStream_t st) {
+    DeviceParticles& g = r->dev;
+    if (!g.valid) return;
+    for (void* p : {(void*)g.pos4, (void*)g.vel4, (void*)g.solid_pos, (void*)g.solid_start})
+        if (p) cudaFreeAsync(p, st);
+    g = DeviceParticles{};
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->staged_total -= r->staged_bytes;
+    r->staged_bytes = 0;
+}
+
+// Uploads a seeded scene into pool memory on the seeding thread's stream, so that admitting it
+// later costs device copies only.  Returns false (and uploads nothing) when it does not fit.
+bool stage(ariel_server* S, Request* r, cudaStream_t st) {
+    const HostParticles& hp = r->hp;
+    const long long n3 = (long long)r->desc.dim * r->desc.dim * r->desc.dim;
+    const long long bytes = 32 * r->np + 16 * r->ns + (hp.solid_start.empty() ? 0 : 4 * (n3 + 1));
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->in_use + S->staged_total + bytes > S->cfg.hbm_budget_bytes) return false;
+        S->staged_total += bytes;
+        r->staged_bytes = bytes;
+    }
+    DeviceParticles g;
+    g.np = r->np;
+    g.ns = r->ns;
+    bool ok = true;
+    auto alloc = [&](void** p, size_t b) {
+        if (ok && cudaMallocFromPoolAsync(p, b ? b : 16, S->pool, st) != cudaSuccess) ok = false;
+    };
+    alloc((void**)&g.pos4, 16 * (size_t)r->np);
+    alloc((void**)&g.vel4, 16 * (size_t)r->np);
+    if (r->ns > 0) alloc((void**)&g.solid_pos, 16 * (size_t)r->ns);
+    if (!hp.solid_start.empty()) alloc((void**)&g.solid_start, 4 * hp.solid_start.size());
+    if (ok && r->np > 0) {
+        ok = cudaMemcpyAsync(g.pos4, hp.pos4.data(), 16 * (size_t)r->np, cudaMemcpyHostToDevice, st) == cudaSuccess &&
+             cudaMemcpyAsync(g.vel4, hp.vel4.data(), 16 * (size_t)r->np, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    }
+    if (ok && r->ns > 0)
+        ok = cudaMemcpyAsync(g.solid_pos, hp.solid_pos.data(), 16 * (size_t)r->ns, cudaMemcpyHostToDevice, st) ==
+             cudaSuccess;
+    if (ok && g.solid_start)
+        ok = cudaMemcpyAsync(g.solid_start, hp.solid_start.data(), 4 * hp.solid_start.size(), cudaMemcpyHostToDevice,
+                             st) == cudaSuccess;
+    if (cudaStreamSynchronize(st) != cudaSuccess) ok = false;
+    g.valid = true;  // so that free_staged releases whatever was allocated
+    r->dev = g;
+    if (!ok) {
+        cudaGetLastError();
+        free_staged(S, r, st);
+        cudaStreamSynchronize(st);
+        return false;
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->staged++;
+    return true;
+}
+
 void prepare_main(ariel_server* S) {
+    cudaSetDevice(S->device);
+    cudaStream_t st = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     for (;;) {
         Request* r = nullptr;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_prep.wait(lk, [&] { return S->stopping || !S->to_prepare.empty(); });
-            if (S->stopping) return;
+            // at most max_ready scenes seeded ahead of admission (host and device memory)
+            S->cv_prep.wait(lk, [&] {
+                return S->stopping ||
+                       (!S->to_prepare.empty() && (int)S->ready.size() + S->preparing < S->cfg.max_ready);
+            });
+            if (S->stopping) break;
             r = S->to_prepare.front();
             S->to_prepare.pop_front();
+            S->preparing++;
         }
         HostParticles hp;
         generate_particles(r->desc, hp);
@@ -118,11 +189,18 @@ void prepare_main(ariel_server* S) {
         const long long bytes = state_bytes({r->desc}, {np}, {ns}, S->prm);
         {
             std::lock_guard<std::mutex> lk(S->mu);
-            r->hp = std::move(hp);
             r->np = np;
             r->ns = ns;
             r->bytes = bytes;
-            if (bytes > S->cfg.hbm_budget_bytes) {
+            r->hp = std::move(hp);
+        }
+        const bool fits = bytes <= S->cfg.hbm_budget_bytes;
+        // the host copy is kept until admission, so an upload can always be dropped again
+        if (fits) stage(S, r, st);
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->preparing--;
+            if (!fits) {
                 // can never fit, even alone
                 r->state = ARIEL_REQ_FAILED;
                 r->status = ARIEL_ERR_OOM;
@@ -137,6 +215,8 @@ void prepare_main(ariel_server* S) {
         }
         S->cv_work.notify_one();
     }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
 }
 
 // Moves the worker's step-time history into the server statistics.
@@ -171,6 +251,10 @@ ariel_status relayout(ariel_server* S, const std::vector<Request*>& retire, cons
     ariel_sim* old = S->batch;
     if (old) {
         if (cudaStreamSynchronize(S->stream) != cudaSuccess) return map_cuda_error(cudaGetLastError(), "batch step");
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->relayout_wait_ms += S->now_ms() - t_begin;
+        }
         ariel_status st = collect_pending(old);
         if (st != ARIEL_OK) return st;
         drain_step_times(S);
@@ -212,6 +296,8 @@ ariel_status relayout(ariel_server* S, const std::vector<Request*>& retire, cons
     if (!retire.empty()) S->cv_done.notify_all();
 
     const int k = (int)(keep.size() + add.size());
+    std::vector<DeviceParticles> staged(k);
+    for (size_t a = 0; a < add.size(); ++a) staged[keep.size() + a] = add[a]->dev;
     std::vector<AsimSceneDesc> descs;
     std::vector<SceneDev> sh;
     std::vector<int64_t> frames;
@@ -238,7 +324,12 @@ ariel_status relayout(ariel_server* S, const std::vector<Request*>& retire, cons
         if (old) free_scratch(old);
         std::vector<HostParticles> hp(k);
         for (size_t a = 0; a < add.size(); ++a) hp[keep.size() + a] = std::move(add[a]->hp);
-        st = build_state(s2, hp, old, &src_idx);
+        const double tb = S->now_ms();
+        st = build_state(s2, hp, old, &src_idx, &staged);
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->relayout_build_ms += S->now_ms() - tb;
+        }
         if (st == ARIEL_OK) st = compute_max_density(s2);
         if (st == ARIEL_OK) st = sort_and_classify_init(s2);
         if (st == ARIEL_OK && cudaStreamSynchronize(S->stream) != cudaSuccess) st = map_cuda_error(cudaGetLastError());
@@ -249,6 +340,10 @@ ariel_status relayout(ariel_server* S, const std::vector<Request*>& retire, cons
         s2->inited = true;
     }
     if (old) delete_sim(old);
+    for (Request* r : add) {
+        free_staged(S, r, S->stream);  // copied into the batch
+        r->hp = HostParticles{};
+    }
     S->batch = s2;
     {
         std::lock_guard<std::mutex> lk(S->mu);
@@ -279,7 +374,8 @@ void worker_main(ariel_server* S) {
             if (S->stopping) break;
             for (Request* r : S->live) (r->steps_done >= r->nsteps ? retire : keep).push_back(r);
             // admission, oldest first, while the new layout fits next to the old persistent state
-            const long long old_keep = S->batch ? bufs_bytes(S->batch, true) : 0;
+            // and the scenes uploaded ahead
+            const long long old_keep = (S->batch ? bufs_bytes(S->batch, true) : 0) + S->staged_total;
             std::vector<AsimSceneDesc> d;
             std::vector<long long> np, ns;
             for (Request* r : keep) {
@@ -296,6 +392,23 @@ void worker_main(ariel_server* S) {
                 if (state_bytes(d, np, ns, S->prm) + old_keep > S->cfg.hbm_budget_bytes) break;
                 add.push_back(r);
                 it = S->ready.erase(it);
+            }
+        }
+        if (!add.empty()) S->cv_prep.notify_all();  // room for more seeding ahead
+        if (add.empty() && retire.empty() && keep.empty() && !S->batch) {
+            // Nothing runs and the oldest waiting scene does not fit next to the scenes uploaded
+            // ahead: drop those uploads (their host copies remain) so that it can be admitted.
+            std::vector<Request*> unstage;
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                if (!S->ready.empty() && S->staged_total > 0)
+                    for (auto& kv : S->ready)
+                        if (kv.second->dev.valid) unstage.push_back(kv.second);
+            }
+            for (Request* r : unstage) free_staged(S, r, S->stream);
+            if (!unstage.empty()) {
+                cudaStreamSynchronize(S->stream);
+                continue;
             }
         }
         if (!retire.empty() || !add.empty()) {
@@ -315,7 +428,13 @@ void worker_main(ariel_server* S) {
             }
         }
         if (!S->batch) continue;
+        const bool first = !S->batch->graph_tried[1] || !S->batch->graph_tried[2];
+        const double tg = S->now_ms();
         ariel_status st = step_async(S->batch);
+        if (first) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->graph_build_ms += S->now_ms() - tg;
+        }
         if (st != ARIEL_OK) {
             fail_live(S, st);
             delete_sim(S->batch);
@@ -379,6 +498,7 @@ ariel_status ariel_server_create(const AsimParams* params, const AsimServerConfi
     S->cfg = *config;
     if (S->cfg.max_live == 0) S->cfg.max_live = 32;
     if (S->cfg.prepare_threads == 0) S->cfg.prepare_threads = 4;
+    if (S->cfg.max_ready <= 0) S->cfg.max_ready = 8;
     S->device = dev;
     if (S->cfg.hbm_budget_bytes == 0) {
         size_t fr = 0, tot = 0;
@@ -400,6 +520,16 @@ ariel_status ariel_server_create(const AsimParams* params, const AsimServerConfi
     }
     uint64_t keep_all = ~0ull;
     cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep_all);
+    if (S->cfg.reserve_budget) {
+        // grow the pool to the whole budget once; it keeps the memory after the free
+        void* p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, (size_t)S->cfg.hbm_budget_bytes, S->pool, S->stream) == cudaSuccess) {
+            cudaFreeAsync(p, S->stream);
+            cudaStreamSynchronize(S->stream);
+        } else {
+            cudaGetLastError();
+        }
+    }
     S->t0 = std::chrono::steady_clock::now();
     ariel_server* raw = S.release();
     for (int i = 0; i < raw->cfg.prepare_threads; ++i) raw->preparers.emplace_back(prepare_main, raw);
@@ -520,6 +650,10 @@ ariel_status ariel_server_stats(ariel_server* S, AsimServerStats* out) {
         out->hbm_peak_bytes = S->peak;
         out->max_live_seen = S->max_live_seen;
         out->last_error = S->last_error;
+        out->relayout_wait_ms = S->relayout_wait_ms;
+        out->relayout_build_ms = S->relayout_build_ms;
+        out->graph_build_ms = S->graph_build_ms;
+        out->staged = S->staged;
         out->timed_steps = (int64_t)steps.size();
     }
     out->wall_ms = S->now_ms();
@@ -542,6 +676,8 @@ ariel_status ariel_server_shutdown(ariel_server* S) {
     if (S->worker.joinable()) S->worker.join();
     for (auto& t : S->preparers)
         if (t.joinable()) t.join();
+    for (auto& kv : S->reqs) free_staged(S, kv.second.get(), S->stream);
+    cudaStreamSynchronize(S->stream);
     {
         std::lock_guard<std::mutex> lk(S->mu);
         for (auto& kv : S->reqs) {

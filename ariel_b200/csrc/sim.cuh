@@ -29,6 +29,17 @@ struct HostParticles {
     bool binned = false;
 };
 
+// One scene's particles and solid bins already in device memory (uploaded ahead of a
+// re-layout by the request server); solid_start is scene-local (n^3 + 1 entries) or null.
+struct DeviceParticles {
+    bool valid = false;
+    float4* pos4 = nullptr;
+    float4* vel4 = nullptr;
+    float4* solid_pos = nullptr;
+    uint32_t* solid_start = nullptr;
+    long long np = 0, ns = 0;
+};
+
 inline float4 pack_vel(float u, float v, float w, int type) {
     float4 r;
     r.x = u;
@@ -114,8 +125,11 @@ void delete_sim(ariel_sim* s);
 // (Re)allocates every buffer for s->descs and uploads the particles.  With `src`, scene i for
 // which (*src_idx)[i] >= 0 takes its particles, pressure warm start, solid bins and solver
 // record from scene (*src_idx)[i] of `src` by device copies instead of from hp[i].
+// With `staged`, scene i whose (*staged)[i].valid takes its particles and solid bins from
+// there by device copies.
 ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ariel_sim* src = nullptr,
-                         const std::vector<int>* src_idx = nullptr);
+                         const std::vector<int>* src_idx = nullptr,
+                         const std::vector<DeviceParticles>* staged = nullptr);
 // Device bytes build_state allocates for these scenes with these particle/solid counts.
 long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector<long long>& particles,
                       const std::vector<long long>& solids, const AsimParams& prm);

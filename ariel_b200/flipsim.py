@@ -236,7 +236,8 @@ class Server:
     """Request server: scenes of any size arrive as (scene, steps) requests and are stepped
     together, re-packed at step boundaries as they arrive and finish (ariel_server_*)."""
 
-    def __init__(self, params=None, hbm_budget_bytes=0, max_live=0, prepare_threads=0, keep_results=1):
+    def __init__(self, params=None, hbm_budget_bytes=0, max_live=0, prepare_threads=0, keep_results=1,
+                 reserve_budget=0):
         self.L = lib()
         if params is None:
             params = A.params_default()
@@ -248,6 +249,7 @@ class Server:
         if prepare_threads:
             cfg.prepare_threads = prepare_threads
         cfg.keep_results = keep_results
+        cfg.reserve_budget = reserve_budget
         h = C.c_void_p()
         check(self.L.ariel_server_create(C.byref(params), C.byref(cfg), C.byref(h)), "ariel_server_create")
         self.h = h

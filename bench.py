@@ -289,7 +289,7 @@ def serve_arm(args, A, prec, ws, rank, pg, gpu_index):
     from ariel_b200.flipsim import Server
     stream = W.arrival_stream(args.rate, args.duration, seed=args.seed + 1000 * rank)
     prm = make_params(A, prec, args.tol)
-    srv = Server(prm, max_live=args.max_live, keep_results=0)
+    srv = Server(prm, max_live=args.max_live, keep_results=0, reserve_budget=1)
     sampler = ClockSampler(gpu_index)
     if pg:
         pg.barrier()
@@ -334,6 +334,9 @@ def serve_arm(args, A, prec, ws, rank, pg, gpu_index):
                     "request_latency_ms_p50": st.latency_ms_p50 if st.finished else None,
                     "request_latency_ms_p99": st.latency_ms_p99 if st.finished else None,
                     "relayouts": st.relayouts, "relayout_ms": st.relayout_ms,
+                    "relayout_wait_ms": st.relayout_wait_ms, "relayout_build_ms": st.relayout_build_ms,
+                    "graph_build_ms": st.graph_build_ms,
+                    "staged": st.staged,
                     "hbm_budget_gb": st.hbm_budget_bytes / 1e9, "hbm_peak_gb": st.hbm_peak_bytes / 1e9,
                     "max_live_seen": st.max_live_seen},
         "step_ms_p50": st.step_ms_p50, "step_ms_p99": st.step_ms_p99,
@@ -370,6 +373,8 @@ def main():
     ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--max-live", type=int, default=32)
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the solve's launch-shape candidates on this workload first and run the fastest")
     ap.add_argument("--precond", choices=["ref", "mic0"], default="ref",
                     help="ref: the reference's preconditioner (solver.inl:104-135); mic0: MIC(0), tau .97")
     args = ap.parse_args()
@@ -417,8 +422,13 @@ def main():
         desc = A.scene_dambreak(args.n, seed=replica_seed(rank))
     barrier = (lambda: pg.barrier()) if pg else None
     sampler = ClockSampler(gpu_index)
-    b, res = run_gpu_pass(A, Batch, desc, make_params(A, prec, args.tol, resample_every=resample_every),
-                          args.steps, args.warmup, sampler, barrier)
+    prm = make_params(A, prec, args.tol, resample_every=resample_every)
+    tune_report = None
+    if args.autotune:
+        from ariel_b200 import autotune
+        prm, tune_report = autotune.tune(desc if isinstance(desc, list) else [desc], prm)
+        prm.timing = 1
+    b, res = run_gpu_pass(A, Batch, desc, prm, args.steps, args.warmup, sampler, barrier)
 
     n_local = res["np"]
     ms, total_particles = aggregate(res["ms"], n_local, pg)
@@ -457,6 +467,8 @@ def main():
                 "final_rel_residual": res["stats"].pcg_rel_residual},
         "roofline": roofline, "clocks": res["clocks"], "gpu_launches": res["launches"],
     }
+    if tune_report is not None:
+        out["autotune"] = tune_report
 
     if not args.no_e2e:
         e2e_ms, h2d, d2h, pinned = run_e2e(b, args.steps)

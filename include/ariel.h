@@ -304,7 +304,11 @@ typedef struct AsimServerConfig {
     int32_t max_live;         /* scenes stepped together at most (<= 1024); 0: 32 */
     int32_t prepare_threads;  /* host threads seeding arriving scenes; 0: 4 */
     int32_t keep_results;     /* 1: keep each finished scene's particles for fetch */
-    int32_t reserved[7];
+    int32_t max_ready;        /* seeded scenes waiting for admission at most (their particles are
+                                 uploaded ahead to device memory when the budget allows); 0: 8 */
+    int32_t reserve_budget;   /* 1: map the whole budget into the server's memory pool at creation,
+                                 so that no re-packing waits for the pool to grow */
+    int32_t reserved[5];
 } AsimServerConfig;
 
 enum { ARIEL_REQ_QUEUED = 0, ARIEL_REQ_READY = 1, ARIEL_REQ_RUNNING = 2, ARIEL_REQ_DONE = 3, ARIEL_REQ_FAILED = 4 };
@@ -334,6 +338,10 @@ typedef struct AsimServerStats {
     int64_t hbm_budget_bytes, hbm_in_use_bytes, hbm_peak_bytes;
     int32_t max_live_seen;
     int32_t last_error;
+    double relayout_wait_ms;  /* part of relayout_ms spent waiting for the batch step in flight */
+    double relayout_build_ms; /* part of relayout_ms spent allocating and filling the new layout */
+    double graph_build_ms;    /* host time capturing and instantiating step graphs */
+    int64_t staged;           /* scenes whose particles were uploaded ahead of admission */
 } AsimServerStats;
 
 void ariel_server_config_default(AsimServerConfig* config);
