@@ -110,6 +110,58 @@ class FlipSim {
     Particles parts_;
 };
 
+// Request server (ariel_server_*): scenes of any size submitted from any thread are stepped
+// together; results are fetched by request id.  No counterpart in the reference.
+class Server {
+   public:
+    explicit Server(const AsimParams* params = nullptr, const AsimServerConfig* config = nullptr) {
+        AsimParams p;
+        if (params)
+            p = *params;
+        else
+            ariel_params_default(&p);
+        AsimServerConfig c;
+        if (config)
+            c = *config;
+        else
+            ariel_server_config_default(&c);
+        check(ariel_server_create(&p, &c, &srv_), "ariel_server_create");
+    }
+    ~Server() {
+        if (srv_) ariel_server_shutdown(srv_);
+    }
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    int64_t Submit(const AsimSceneDesc& scene, int32_t nsteps) {
+        int64_t id = 0;
+        check(ariel_server_submit(srv_, &scene, nsteps, &id), "ariel_server_submit");
+        return id;
+    }
+    AsimRequestInfo Poll(int64_t id) {
+        AsimRequestInfo info;
+        check(ariel_server_poll(srv_, id, &info), "ariel_server_poll");
+        return info;
+    }
+    void Wait(int64_t id, double timeout_ms = 1.0e9) { check(ariel_server_wait(srv_, id, timeout_ms), "ariel_server_wait"); }
+    void Drain(double timeout_ms = 1.0e9) { check(ariel_server_drain(srv_, timeout_ms), "ariel_server_drain"); }
+    // Positions and velocities of a finished request, id order, xyz-interleaved.
+    void Fetch(int64_t id, std::vector<float>& pos, std::vector<float>& vel) {
+        const AsimRequestInfo info = Poll(id);
+        pos.resize(3 * (size_t)info.n_particles);
+        vel.resize(3 * (size_t)info.n_particles);
+        check(ariel_server_fetch(srv_, id, pos.data(), vel.data()), "ariel_server_fetch");
+    }
+    AsimServerStats Stats() {
+        AsimServerStats st;
+        check(ariel_server_stats(srv_, &st), "ariel_server_stats");
+        return st;
+    }
+
+   private:
+    ariel_server* srv_ = nullptr;
+};
+
 }  // namespace ariel
 
 #endif

@@ -31,3 +31,4 @@ def test_cpp_wrapper_steps(tmp_path):
     r = subprocess.run([_build(tmp_path), "16", "3"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "frame 3 particles 7904" in r.stdout
+    assert "served identical, second request 4 steps" in r.stdout
