@@ -47,6 +47,9 @@ SIGNATURES = {
     "ariel_kernel_launches": ([], C.c_int64),
     "ariel_last_error": ([], C.c_char_p),
     "ariel_sort_by_cell_noalloc": ([_vp, C.c_int64, C.c_int32, _vp, _vp, _vp, _vp], C.c_int),
+    "ariel_checkpoint_save": ([_vp, C.c_char_p], C.c_int),
+    "ariel_checkpoint_load": ([_vp, C.c_char_p], C.c_int),
+    "ariel_export_particles": ([_vp, C.c_int32, C.c_char_p, C.c_int32], C.c_int),
     "ariel_server_config_default": ([C.POINTER(A.AsimServerConfig)], None),
     "ariel_server_create": ([C.POINTER(A.AsimParams), C.POINTER(A.AsimServerConfig), C.POINTER(_vp)], C.c_int),
     "ariel_server_submit": ([_vp, C.POINTER(A.AsimSceneDesc), C.c_int32, C.POINTER(C.c_int64)], C.c_int),

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -1421,6 +1422,146 @@ ariel_status ariel_selftest_barrier_timeout(double timeout_ms) {
     cudaFree(err);
     if (e != cudaSuccess) return map_cuda_error(e);
     return h ? ARIEL_ERR_DEVICE_TIMEOUT : ARIEL_OK;
+}
+
+// ---- checkpoints -------------------------------------------------------------------------
+// File: "ARIELCK1", int32 k, then per scene: AsimSceneDesc, int64 frame, float max_density,
+// int64 particles, pos4[particles], vel4[particles] (float4), P[n^3] (float), P64[n^3] (double).
+// That is every piece of state a step reads from the previous one (the particles, the pressure
+// warm start, the frame counter that keys the resampling RNG, and the density normaliser), so a
+// handle loaded from a checkpoint continues bit-identically.
+static const char kCkMagic[8] = {'A', 'R', 'I', 'E', 'L', 'C', 'K', '1'};
+
+ariel_status ariel_checkpoint_save(ariel_sim* s, const char* path) {
+    if (!s || !path) return ARIEL_ERR_INVALID_ARG;
+    if (!s->inited) return ARIEL_ERR_STATE;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    ARIEL_TRY(refresh_scene_table(s));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return ARIEL_ERR_INVALID_ARG;
+    bool ok = std::fwrite(kCkMagic, 1, 8, f) == 8;
+    const int32_t k = s->k;
+    ok = ok && std::fwrite(&k, sizeof(k), 1, f) == 1;
+    for (int i = 0; ok && i < k; ++i) {
+        const long long pb = s->ppref[i], np = s->ppref[i + 1] - pb;
+        const long long cb = s->cpref[i], nc = s->cpref[i + 1] - cb;
+        const int64_t frame = s->sh[i].frame;
+        const float md = s->sh[i].max_density;
+        std::vector<float4> p4(np), v4(np);
+        std::vector<float> P(nc);
+        std::vector<double> P64(nc);
+        if (np > 0) {
+            ARIEL_CUDA(copy_sync(s->stream, p4.data(), s->S.pos4 + pb, np * sizeof(float4), cudaMemcpyDeviceToHost));
+            ARIEL_CUDA(copy_sync(s->stream, v4.data(), s->S.vel4 + pb, np * sizeof(float4), cudaMemcpyDeviceToHost));
+        }
+        ARIEL_CUDA(copy_sync(s->stream, P.data(), s->S.P + cb, nc * sizeof(float), cudaMemcpyDeviceToHost));
+        ARIEL_CUDA(copy_sync(s->stream, P64.data(), s->S.P64 + cb, nc * sizeof(double), cudaMemcpyDeviceToHost));
+        const int64_t n64 = np;
+        ok = std::fwrite(&s->descs[i], sizeof(AsimSceneDesc), 1, f) == 1 && std::fwrite(&frame, 8, 1, f) == 1 &&
+             std::fwrite(&md, 4, 1, f) == 1 && std::fwrite(&n64, 8, 1, f) == 1 &&
+             std::fwrite(p4.data(), sizeof(float4), np, f) == (size_t)np &&
+             std::fwrite(v4.data(), sizeof(float4), np, f) == (size_t)np &&
+             std::fwrite(P.data(), sizeof(float), nc, f) == (size_t)nc &&
+             std::fwrite(P64.data(), sizeof(double), nc, f) == (size_t)nc;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
+}
+
+ariel_status ariel_checkpoint_load(ariel_sim* s, const char* path) {
+    if (!s || !path) return ARIEL_ERR_INVALID_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return ARIEL_ERR_INVALID_ARG;
+    char magic[8];
+    int32_t k = 0;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCkMagic, 8) == 0 &&
+              std::fread(&k, sizeof(k), 1, f) == 1 && k == s->k;
+    std::vector<HostParticles> hp(ok ? k : 0);
+    std::vector<std::vector<float>> P(hp.size());
+    std::vector<std::vector<double>> P64(hp.size());
+    std::vector<int64_t> frames(hp.size());
+    std::vector<float> md(hp.size());
+    for (int i = 0; ok && i < k; ++i) {
+        AsimSceneDesc d;
+        int64_t np = 0;
+        ok = std::fread(&d, sizeof(d), 1, f) == 1 && std::fread(&frames[i], 8, 1, f) == 1 &&
+             std::fread(&md[i], 4, 1, f) == 1 && std::fread(&np, 8, 1, f) == 1 && np >= 0 && np < (1ll << 31);
+        // the checkpoint must describe the same scenes as the handle
+        ok = ok && std::memcmp(&d, &s->descs[i], sizeof(d)) == 0;
+        if (!ok) break;
+        const long long nc = (long long)d.dim * d.dim * d.dim;
+        hp[i].pos4.resize(np);
+        hp[i].vel4.resize(np);
+        P[i].resize(nc);
+        P64[i].resize(nc);
+        ok = std::fread(hp[i].pos4.data(), sizeof(float4), np, f) == (size_t)np &&
+             std::fread(hp[i].vel4.data(), sizeof(float4), np, f) == (size_t)np &&
+             std::fread(P[i].data(), sizeof(float), nc, f) == (size_t)nc &&
+             std::fread(P64[i].data(), sizeof(double), nc, f) == (size_t)nc;
+    }
+    std::fclose(f);
+    if (!ok) return ARIEL_ERR_INVALID_ARG;
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < k; ++i) {
+        s->sh[i].frame = frames[i];
+        s->sh[i].max_density = md[i];
+        s->frames[i] = frames[i];
+    }
+    ARIEL_TRY(build_state(s, hp));
+    for (int i = 0; i < k; ++i) {
+        const long long cb = s->cpref[i], nc = s->cpref[i + 1] - cb;
+        ARIEL_CUDA(copy_sync(s->stream, s->S.P + cb, P[i].data(), nc * sizeof(float), cudaMemcpyHostToDevice));
+        ARIEL_CUDA(copy_sync(s->stream, s->S.P64 + cb, P64[i].data(), nc * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    ARIEL_TRY(sort_and_classify_init(s));
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    s->inited = true;
+    return ARIEL_OK;
+}
+
+// ---- particle export (Scene::ExportParticles' Partio branch, src/scene/scene.cpp:35-80) ----
+// FLUID particles in id order with attributes position (grid units: unit position x maxd), v
+// and id (their index in the export), to `path` with the four-digit frame inserted before the
+// extension (".gz" counted as part of it).  Written in Houdini's classic ASCII geometry form
+// (the ".geo" one of Partio's formats); other extensions are refused.
+ariel_status ariel_export_particles(ariel_sim* s, int32_t scene, const char* path, int32_t frame) {
+    if (!s || !path || scene < 0 || scene >= s->k || frame < 0) return ARIEL_ERR_INVALID_ARG;
+    std::string name(path);
+    const size_t slash = name.find_last_of('/');
+    const size_t dot = name.find_last_of('.');
+    if (dot == std::string::npos || (slash != std::string::npos && dot < slash)) return ARIEL_ERR_INVALID_ARG;
+    std::string ext = name.substr(dot);
+    std::string stem = name.substr(0, dot);
+    if (ext == ".gz") return ARIEL_ERR_INVALID_ARG;  // compressed output is not written
+    if (ext != ".geo") return ARIEL_ERR_INVALID_ARG;
+    char fr[16];
+    std::snprintf(fr, sizeof(fr), ".%04d", frame);
+    const std::string out = stem + fr + ext;
+    const long long b = s->ppref[scene], n = s->ppref[scene + 1] - b;
+    std::vector<float4> p4(n), v4(n);
+    ARIEL_CUDA(cudaStreamSynchronize(s->stream));
+    if (n > 0) {
+        ARIEL_CUDA(copy_sync(s->stream, p4.data(), s->S.pos4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+        ARIEL_CUDA(copy_sync(s->stream, v4.data(), s->S.vel4 + b, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
+    const float maxd = s->sh[scene].maxd;
+    std::vector<long long> fluid;
+    for (long long i = 0; i < n; ++i)
+        if (type_bits(v4[i]) == ARIEL_FLUID) fluid.push_back(i);
+    FILE* f = std::fopen(out.c_str(), "w");
+    if (!f) return ARIEL_ERR_INVALID_ARG;
+    std::fprintf(f, "PGEOMETRY V5\nNPoints %lld NPrims 1\nNPointGroups 0 NPrimGroups 0\n", (long long)fluid.size());
+    std::fprintf(f, "NPointAttrib 2 NVertexAttrib 0 NPrimAttrib 0 NAttrib 0\nPointAttrib\n");
+    std::fprintf(f, "v 3 vector 0 0 0\nid 1 int 0\n");
+    for (size_t e = 0; e < fluid.size(); ++e) {
+        const float4& p = p4[fluid[e]];
+        const float4& v = v4[fluid[e]];
+        std::fprintf(f, "%.9g %.9g %.9g 1 (%.9g %.9g %.9g %zu)\n", p.x * maxd, p.y * maxd, p.z * maxd, v.x, v.y, v.z, e);
+    }
+    std::fprintf(f, "Part %lld", (long long)fluid.size());
+    for (size_t e = 0; e < fluid.size(); ++e) std::fprintf(f, " %zu", e);
+    std::fprintf(f, "\nbeginExtra\nendExtra\n");
+    return std::fclose(f) == 0 ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
 }
 
 int64_t ariel_kernel_launches(void) { return launch_count(); }

@@ -161,6 +161,18 @@ class Batch:
         return dict(stage_ms=ms, solve_kernel_ms=solve_k.value, steps=n.value,
                     step_ms=steps[:min(n.value, max_steps)].copy())
 
+    def checkpoint_save(self, path):
+        check(self.L.ariel_checkpoint_save(self.h, str(path).encode()), "ariel_checkpoint_save")
+
+    def checkpoint_load(self, path):
+        check(self.L.ariel_checkpoint_load(self.h, str(path).encode()), "ariel_checkpoint_load")
+
+    def export_particles(self, path, frame, scene=0):
+        """Scene::ExportParticles' particle file (Houdini ASCII .geo); returns the written path."""
+        check(self.L.ariel_export_particles(self.h, scene, str(path).encode(), frame), "ariel_export_particles")
+        stem, ext = str(path).rsplit(".", 1)
+        return "%s.%04d.%s" % (stem, frame, ext)
+
     def solver_totals(self, scene=0):
         t = A.AsimSolverTotals()
         check(self.L.ariel_solver_totals(self.h, scene, C.byref(t)), "ariel_solver_totals")

@@ -264,6 +264,18 @@ ariel_status ariel_timing_get(ariel_sim* sim, double* ms, double* solve_kernel_m
  * worked and ARIEL_OK if the barrier (wrongly) completed. */
 ariel_status ariel_selftest_barrier_timeout(double timeout_ms);
 
+/* Checkpoints: every piece of state a step reads from the previous one (particles, pressure
+ * warm start, frame counter, density normaliser) of every scene of the handle, in one file.
+ * Loading needs a handle created with the same scene descriptions and continues
+ * bit-identically.  Replaces no reference function: the reference's only output is the particle
+ * export below. */
+ariel_status ariel_checkpoint_save(ariel_sim* sim, const char* path);
+ariel_status ariel_checkpoint_load(ariel_sim* sim, const char* path);
+/* Scene::ExportParticles' particle branch (src/scene/scene.cpp:35-80): FLUID particles with
+ * position (grid units), v and id, to `path` with ".%04d" of `frame` inserted before the
+ * extension.  Written as Houdini classic ASCII geometry; `path` must end in ".geo". */
+ariel_status ariel_export_particles(ariel_sim* sim, int32_t scene, const char* path, int32_t frame);
+
 /* Count of this library's kernel launches issued so far (all handles). */
 int64_t ariel_kernel_launches(void);
 

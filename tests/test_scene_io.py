@@ -1,0 +1,119 @@
+"""Scene files, checkpoints and particle export.
+
+- The reference's JSON scenes (SceneLoader) map onto AsimSceneDesc; a file describing the
+  benchmark dam break gives the same seeded particles as the built-in description.
+- A checkpoint holds everything a step reads from the previous one: a handle loaded from it
+  continues bit-identically.
+- The particle export (Scene::ExportParticles' Partio branch) writes FLUID particles with
+  position in grid units, v and id, under the frame-numbered name.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ariel_b200 import _abi as A
+from ariel_b200.flipsim import Batch, state_bytes
+from ariel_b200.sceneloader import SceneError, load_scene
+
+from helpers import assert_bits, dambreak, params
+
+
+def _scene_json(n=64, rotation=None, meshfile=None, dim=None):
+    box = {"id": "tank", "mesh_gen": "box", "point0": {"x": 0, "y": 0, "z": 0},
+           "point1": {"x": 0.4 * n, "y": 0.6 * n, "z": 1.0 * n}}
+    ball = {"id": "ball", "mesh_gen": "sphere", "center": {"x": 0, "y": 0, "z": 0}, "radius": 0.15 * n}
+    moved = {"id": "moved", "translation": {"x": 0.6 * n, "y": 0.3 * n, "z": 0.5 * n}}
+    if rotation:
+        moved["rotation"] = rotation
+    return {
+        "settings": [{"density": 0.5, "step_size": 1.0 / 480.0,
+                      "dim": dim or {"x": n, "y": n, "z": n}, "partio_output": "out/particles.geo"}],
+        "camera": [{"resolution": {"x": 640, "y": 480}}],
+        "globalforces": [{"x": 0.0, "y": -9.8, "z": 0.0}],
+        "transforms": [{"id": "identity"}, moved],
+        "meshfiles": [meshfile or box, ball],
+        "geoms": [{"id": "water", "type": "mesh", "geom_frames": ["tank"], "transform_frames": ["identity"]},
+                  {"id": "rock", "type": "mesh", "geom_frames": ["ball"], "transform_frames": ["moved"]}],
+        "sim": [{"geom": "water", "type": "liquid"}, {"geom": "rock", "type": "solid"}],
+    }
+
+
+def test_scene_file_matches_builtin_description(tmp_path):
+    p = tmp_path / "dambreak.json"
+    p.write_text(json.dumps(_scene_json(64)))
+    d, info = load_scene(str(p))
+    ref = A.scene_dambreak(64, liquid_hi=(0.4, 0.6, 1.0), dt=1.0 / 480.0, seed=1, jitter=0.0,
+                           spheres=[((0.6, 0.3, 0.5), 0.15)])
+    assert info["dim"] == 64 and info["partio_output"] == "out/particles.geo"
+    assert d.dim == ref.dim and d.density == ref.density and d.stepsize == ref.stepsize
+    assert d.n_forces == 1 and abs(d.forces[0][1] + 9.8) < 1e-6
+    assert d.n_liquid == 1 and d.n_solid == 1 and d.jitter == 0.0
+    for a in range(3):
+        assert abs(d.liquid[0].hi[a] - ref.liquid[0].hi[a]) < 1e-7
+        assert abs(d.solid[0].center[a] - ref.solid[0].center[a]) < 1e-7
+    assert abs(d.solid[0].radius - ref.solid[0].radius) < 1e-7
+    # the seeded lattice (host-side) is the same: equal device footprints, particle for particle
+    prm = params(precision=A.PREC_MIXED)
+    assert state_bytes([d], prm) == state_bytes([ref], prm)
+
+
+@pytest.mark.parametrize("bad", ["rotation", "file", "grid"])
+def test_scene_file_refuses_what_it_cannot_represent(tmp_path, bad):
+    kw = {"rotation": dict(rotation={"x": 0, "y": 30, "z": 0}),
+          "file": dict(meshfile={"id": "tank", "file": "tank.obj"}),
+          "grid": dict(dim={"x": 64, "y": 32, "z": 64})}[bad]
+    p = tmp_path / "bad.json"
+    p.write_text(json.dumps(_scene_json(64, **kw)))
+    with pytest.raises(SceneError):
+        load_scene(str(p))
+
+
+@pytest.mark.gpu
+def test_checkpoint_continues_bit_identically(tmp_path):
+    descs = [dambreak(16, seed=1), dambreak(20, seed=3, spheres=[((0.6, 0.3, 0.5), 0.15)])]
+    prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1)
+    a = Batch(descs, prm)
+    a.init()
+    a.step(4)
+    ck = tmp_path / "state.ck"
+    a.checkpoint_save(ck)
+    a.step(3)
+    b = Batch(descs, prm)
+    b.checkpoint_load(ck)
+    assert b.stats(1).frame == 4
+    b.step(3)
+    for i in range(2):
+        pa, pb = a.get_particles(i), b.get_particles(i)
+        assert_bits("scene %d pos" % i, pb["pos"], pa["pos"])
+        assert_bits("scene %d vel" % i, pb["vel"], pa["vel"])
+        assert_bits("scene %d P" % i, b.get_grid(A.GRID_P, i), a.get_grid(A.GRID_P, i))
+    other = Batch([dambreak(16, seed=2)], prm)
+    with pytest.raises(Exception):
+        other.checkpoint_load(ck)
+    for h in (a, b, other):
+        h.close()
+
+
+@pytest.mark.gpu
+def test_particle_export(tmp_path):
+    d = dambreak(16, seed=1, spheres=[((0.6, 0.3, 0.5), 0.15)])
+    b = Batch([d], params())
+    b.init()
+    b.step(2)
+    path = b.export_particles(tmp_path / "parts.geo", 7)
+    assert os.path.basename(path) == "parts.0007.geo"
+    st = b.get_particles()
+    b.close()
+    fl = st["type"] == A.FLUID
+    lines = open(path).read().splitlines()
+    assert lines[0] == "PGEOMETRY V5"
+    assert lines[1] == "NPoints %d NPrims 1" % fl.sum()
+    rows = [l for l in lines if l.endswith(")") and "(" in l]
+    assert len(rows) == fl.sum()
+    pos = np.array([[float(x) for x in r.split("(")[0].split()[:3]] for r in rows], np.float32)
+    rest = np.array([[float(x) for x in r.split("(")[1].rstrip(")").split()] for r in rows])
+    np.testing.assert_array_equal(pos, st["pos"][fl] * np.float32(16))
+    np.testing.assert_array_equal(rest[:, :3].astype(np.float32), st["vel"][fl])
+    np.testing.assert_array_equal(rest[:, 3], np.arange(fl.sum()))
