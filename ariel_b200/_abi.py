@@ -138,7 +138,7 @@ def params_default():
     p.stop_rule = STOP_REF_ABS
     p.max_iters = 0
     p.tol = 1e-5
-    p.inner_tol = 1e-4
+    p.inner_tol = 1e-6
     p.max_outer = 8
     p.resample_every = 1
     p.mic_tau = 0.97

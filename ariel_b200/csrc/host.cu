@@ -548,7 +548,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     // which only the device knows; keep launching it (it returns at once when not needed)
     A.may_be_ordered = 1;
     A.tol = s->prm.tol;
-    A.inner_tol = s->prm.inner_tol > 0 ? s->prm.inner_tol : 1e-4;
+    A.inner_tol = s->prm.inner_tol > 0 ? s->prm.inner_tol : 1e-6;
     A.tau = s->prm.mic_tau;
     A.sigma = s->prm.mic_sigma;
     double tmo_ms = s->prm.barrier_timeout_ms > 0 ? s->prm.barrier_timeout_ms : 2000.0;
@@ -1003,7 +1003,7 @@ void ariel_params_default(AsimParams* p) {
     p->stop_rule = ARIEL_STOP_REF_ABS;
     p->max_iters = 0;
     p->tol = 1e-5;
-    p->inner_tol = 1e-4;
+    p->inner_tol = 1e-6;  // deep enough that one fp32 correction solve usually meets the target, shallow enough for fp32 to reach
     p->max_outer = 8;
     p->resample_every = 1;  // flip.cpp:121
     p->mic_tau = 0.97;

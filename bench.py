@@ -129,6 +129,7 @@ def load_traffic(workload):
 
 
 PRECOND = "ref"
+INNER_TOL = 0.0
 
 
 def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
@@ -140,6 +141,8 @@ def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
     p.use_graph = graph
     p.timing = timing
     p.resample_every = resample_every
+    if INNER_TOL > 0:
+        p.inner_tol = INNER_TOL
     return p
 
 
@@ -382,9 +385,12 @@ def main():
                     help="time the solve's launch-shape candidates on this workload first and run the fastest")
     ap.add_argument("--precond", choices=["ref", "mic0"], default="ref",
                     help="ref: the reference's preconditioner (solver.inl:104-135); mic0: MIC(0), tau .97")
+    ap.add_argument("--inner-tol", type=float, default=0.0,
+                    help="MIXED: relative reduction asked of each fp32 correction solve (0: library default)")
     args = ap.parse_args()
-    global PRECOND
+    global PRECOND, INNER_TOL
     PRECOND = args.precond
+    INNER_TOL = args.inner_tol
     if args.workload == "sphere" and args.n == 128:
         args.n = 256
     if args.warmup < 3 and args.impl == "ours":

@@ -143,7 +143,7 @@ typedef struct AsimParams {
     int32_t stop_rule;        /* ARIEL_STOP_* */
     int32_t max_iters;        /* PCG iteration cap; 0 -> n^3 (solver.inl:325) */
     double tol;               /* relative tolerance for ARIEL_STOP_REL */
-    double inner_tol;         /* MIXED: relative reduction asked of each fp32 inner solve */
+    double inner_tol;         /* MIXED: relative reduction asked of each fp32 inner solve (1e-6) */
     int32_t max_outer;        /* MIXED: cap on refinement sweeps */
     int32_t resample_every;   /* resample every k-th step; 1 = every step as the reference
                                  (flip.cpp:121); 0 = never */
