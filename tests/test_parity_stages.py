@@ -15,11 +15,7 @@ from ariel_b200 import _abi as A
 from ariel_b200.flipsim import Batch
 from oracle.pyoracle import RefSim
 
-from helpers import assert_bits, assert_close, dambreak, evolved_state, params
-
-FACE_GRIDS = (A.GRID_UX, A.GRID_UY, A.GRID_UZ)
-PREV_GRIDS = (A.GRID_PREV_UX, A.GRID_PREV_UY, A.GRID_PREV_UZ)
-CELL_GRIDS = (A.GRID_D, A.GRID_L)
+from helpers import assert_bits, dambreak, evolved_state, params, stage_parity
 
 CASES = [
     ("dambreak16_fresh", dambreak(16, seed=3), 0),
@@ -42,12 +38,6 @@ def _pair(desc, steps, prm):
     return ora, gpu
 
 
-def _particles(tag, g, o, fields=("pos", "vel", "mass", "type")):
-    gp, op = g.get_particles(), o.get_particles()
-    for f in fields:
-        assert_bits("%s %s" % (tag, f), gp[f], op[f])
-
-
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,desc,steps", CASES, ids=[c[0] for c in CASES])
 def test_stage_parity(name, desc, steps):
@@ -55,43 +45,7 @@ def test_stage_parity(name, desc, steps):
     prm = params(stop=A.STOP_REL, tol=1e-6)
     ora, gpu = _pair(desc, steps, prm)
     assert gpu.max_density() == ora.max_density()
-    for stage in range(A.STAGE_COUNT):
-        ora.stage(stage)
-        gpu.stage(stage)
-        tag = "%s/%s" % (name, A.STAGE_NAMES[stage])
-        if stage in (A.STAGE_BEGIN, A.STAGE_FORCES, A.STAGE_G2P_ADVECT, A.STAGE_RESAMPLE):
-            _particles(tag, gpu, ora)
-        elif stage == A.STAGE_SORT:
-            gc, gn = gpu.get_cells()
-            oc, on = ora.get_cells()
-            assert_bits(tag + " particle->cell", gc, oc)
-            assert_bits(tag + " per-cell counts", gn, on)
-        elif stage == A.STAGE_DENSITY:
-            assert_bits(tag + " density", gpu.get_particles()["density"], ora.get_particles()["density"])
-        elif stage == A.STAGE_P2G:
-            for w in FACE_GRIDS:
-                assert_bits("%s face %d" % (tag, w), gpu.get_grid(w), ora.get_grid(w))
-        elif stage == A.STAGE_CLASSIFY:
-            assert_bits(tag + " flags", gpu.get_grid(A.GRID_A), ora.get_grid(A.GRID_A))
-            assert_bits(tag + " L", gpu.get_grid(A.GRID_L), ora.get_grid(A.GRID_L))
-        elif stage == A.STAGE_BOUNDARY_DIV:
-            for w in FACE_GRIDS + PREV_GRIDS:
-                assert_bits("%s grid %d" % (tag, w), gpu.get_grid(w), ora.get_grid(w))
-            assert_bits(tag + " D", gpu.get_grid(A.GRID_D), ora.get_grid(A.GRID_D))
-        elif stage == A.STAGE_SOLVE:
-            Pg, Po = gpu.get_grid(A.GRID_P), ora.get_grid(A.GRID_P)
-            flags = ora.get_grid(A.GRID_A)
-            fl = flags == A.FLUID
-            assert (Pg[~fl] == 0).all() and (Po[~fl] == 0).all()
-            sg, so = gpu.stats(), ora.stats()
-            assert sg.pcg_converged and so.pcg_converged
-            scale = np.abs(Po[fl]).max() + 1e-30
-            assert_close(tag + " P", Pg[fl] / scale, Po[fl] / scale, rtol=0, atol=1e-3)
-            # identical inputs for the following stages
-            gpu.set_grid(A.GRID_P, Po)
-        elif stage in (A.STAGE_GRADIENT, A.STAGE_EXTRAPOLATE):
-            for w in FACE_GRIDS + PREV_GRIDS:
-                assert_bits("%s grid %d" % (tag, w), gpu.get_grid(w), ora.get_grid(w))
+    stage_parity(name, gpu, ora)
     ora.close()
     gpu.close()
 
