@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -858,6 +859,12 @@ ariel_status collect_step_events(ariel_sim* s, int slot) {
 
 // which: 0 plain step, 1/2 step recording event set 0/1.
 void try_build_graph(ariel_sim* s, int which) {
+    const auto t_start = std::chrono::steady_clock::now();
+    struct Timer {
+        ariel_sim* s;
+        std::chrono::steady_clock::time_point t;
+        ~Timer() { s->graph_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count(); }
+    } timer{s, t_start};
     s->graph_tried[which] = true;
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {

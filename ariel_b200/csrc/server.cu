@@ -428,12 +428,11 @@ void worker_main(ariel_server* S) {
             }
         }
         if (!S->batch) continue;
-        const bool first = !S->batch->graph_tried[1] || !S->batch->graph_tried[2];
-        const double tg = S->now_ms();
+        const double g0 = S->batch->graph_ms;
         ariel_status st = step_async(S->batch);
-        if (first) {
+        {
             std::lock_guard<std::mutex> lk(S->mu);
-            S->graph_build_ms += S->now_ms() - tg;
+            S->graph_build_ms += S->batch->graph_ms - g0;
         }
         if (st != ARIEL_OK) {
             fail_live(S, st);

@@ -102,6 +102,7 @@ struct ariel_sim {
     float* d_stage = nullptr;  // xyz staging for host-buffer particle I/O
     int last_status = ARIEL_OK;
     std::vector<int64_t> frames;
+    double graph_ms = 0;  // host time spent capturing and instantiating step graphs
 };
 
 namespace ariel {
