@@ -512,7 +512,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
     const float maxd = D.maxd;
     const float dt = D.dt;
     const float re = D.resample_re;
-    const float near2 = 2.0f * re * re;  // beyond this the spring term is exactly zero
+    // Beyond re the Smooth weight is 0 (dist*dist, with dist the rounded root of d2, reaches
+    // re^2 once d2 exceeds it by a few ulp), and a zero weight adds +-0, which leaves the target
+    // position unchanged; the 1% margin covers that rounding.  Draws for the jitter branch
+    // (dist <= 0.1 re) are inside the radius, so their order is unchanged.
+    const float near2 = 1.01f * re * re;
     const uint32_t gid = (uint32_t)(S.sid[s] - D.p_begin);
     uint32_t draws = 0;
     float3 spring = make_float3(0, 0, 0);
