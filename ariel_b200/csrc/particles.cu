@@ -493,11 +493,11 @@ __device__ __forceinline__ void axis_cells(float x, int c, int n, float ch, floa
 }
 
 // The resampler runs as two kernels over the slots of its own Sort: springs (the target
-// position t), then the velocity at t and the acceptance.  In both, each thread walks the 27
-// neighbour cells of the reference (threads of one cell share them, so a warp stays
-// together) testing only distance, records the few candidates in ascending slot order --
-// the reference's summation order -- and then evaluates them with the reference's exact
-// arithmetic.  Neighbours that fail the test contribute exactly nothing.
+// position t), then the velocity at t and the acceptance.  In both, each thread walks those of
+// the reference's 27 neighbour cells that reach within the kernel radius (about half a cell,
+// so usually 2 per axis), testing only distance, records the few candidates in ascending slot
+// order -- the reference's summation order -- and then evaluates them with the reference's
+// exact arithmetic.  Neighbours outside the radius contribute exactly nothing.
 __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
     SCENE_PREFIX(S.p_pref);
     __shared__ uint32_t lst[kResList][kBlock];
@@ -545,9 +545,19 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
         }
     };
     int xl, xh, yl, yh, zl, zh;
-    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.x)), n, xl, xh);
-    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.y)), n, yl, yh);
-    nb_range(gmax(0.0f, gmin(maxd, maxd * p4.z)), n, zl, zh);
+    {
+        const float gx = gmax(0.0f, gmin(maxd, maxd * p4.x)), gy = gmax(0.0f, gmin(maxd, maxd * p4.y)),
+                    gz = gmax(0.0f, gmin(maxd, maxd * p4.z));
+        nb_range(gx, n, xl, xh);
+        nb_range(gy, n, yl, yh);
+        nb_range(gz, n, zl, zh);
+        // of the reference's 27 cells, only those within the candidate radius (5% margin
+        // over the test below, for the rounding of the cell boxes)
+        const float ch = 1.0f / maxd, lim = 1.05f * near2;
+        axis_cells(p4.x, min((int)gx, n - 1), n, ch, lim, xl, xh);
+        axis_cells(p4.y, min((int)gy, n - 1), n, ch, lim, yl, yh);
+        axis_cells(p4.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
+    }
     int nl = 0;
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
@@ -606,9 +616,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
         wsum += w;
     };
     int xl, xh, yl, yh, zl, zh;
-    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.x)), n, xl, xh);
-    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.y)), n, yl, yh);
-    nb_range(gmax(0.0f, gmin(maxd - 1, maxd * t.z)), n, zl, zh);
+    {
+        const float gx = gmax(0.0f, gmin(maxd - 1, maxd * t.x)), gy = gmax(0.0f, gmin(maxd - 1, maxd * t.y)),
+                    gz = gmax(0.0f, gmin(maxd - 1, maxd * t.z));
+        nb_range(gx, n, xl, xh);
+        nb_range(gy, n, yl, yh);
+        nb_range(gz, n, zl, zh);
+        const float ch = 1.0f / maxd, lim = 1.05f * re2;
+        axis_cells(t.x, min((int)gx, n - 1), n, ch, lim, xl, xh);
+        axis_cells(t.y, min((int)gy, n - 1), n, ch, lim, yl, yh);
+        axis_cells(t.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
+    }
     int nl = 0;
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
