@@ -227,6 +227,37 @@ def cpu_baseline_sample(A, desc, tol, faithful=True, max_steps=1):
     return n, dt, cores, st
 
 
+def fp64_oracle_error(A, Batch, b, desc, tols=(1e-5, 1e-7)):
+    """Error of the MIXED solve against a tight FP64 CPU solve (the oracle, as the checker) on the
+    bench's own last pressure system (flags, liquid SDF and divergence of its final step), each
+    tolerance solved from a zero start: |P - P*| / |P*| over FLUID cells."""
+    import numpy as np
+    from oracle.pyoracle import solve_fp64
+    n = desc.dim
+    flags, L, D = b.get_grid(A.GRID_A), b.get_grid(A.GRID_L), b.get_grid(A.GRID_D)
+    fl = flags == A.FLUID
+    t0 = time.perf_counter()
+    xstar, it, rel = solve_fp64(n, flags, L, D.astype(np.float64).ravel(), tol=1e-12)
+    out = {"oracle": {"tol": 1e-12, "iterations": it, "rel_residual": rel, "seconds": time.perf_counter() - t0},
+           "fluid_cells": int(fl.sum())}
+    p = b.get_particles()
+    zeros = np.zeros((n, n, n), np.float32)
+    for tol in tols:
+        g = Batch([desc], make_params(A, A.PREC_MIXED, tol, timing=0, graph=0))
+        g.set_particles(p["pos"], p["vel"], p["mass"], p["type"])
+        for w, arr in ((A.GRID_A, flags), (A.GRID_L, L), (A.GRID_D, D), (A.GRID_P, zeros)):
+            g.set_grid(w, arr)
+        g.set_grid(A.GRID_P64, zeros.astype(np.float64))
+        g.stage(A.STAGE_SOLVE)
+        x = g.get_grid(A.GRID_P64)
+        st = g.stats()
+        err = float(np.linalg.norm((x - xstar)[fl]) / max(np.linalg.norm(xstar[fl]), 1e-300))
+        out["tol_%g" % tol] = {"rel_error": err, "iterations": st.pcg_iterations, "sweeps": st.pcg_outer,
+                               "rel_residual": st.pcg_rel_residual}
+        g.close()
+    return out
+
+
 def reference_arm(args, A, ws, rank):
     if rank != 0:
         return 0
@@ -481,6 +512,9 @@ def main():
     }
     if tune_report is not None:
         out["autotune"] = tune_report
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "dambreak":
+        out["pcg"]["fp64_oracle_error"] = fp64_oracle_error(A, Batch, b, desc)
 
     if not args.no_e2e:
         e2e_ms, h2d, d2h, pinned = run_e2e(b, args.steps)
