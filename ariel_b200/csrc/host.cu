@@ -800,7 +800,12 @@ using namespace ariel::hostimpl;
 
 namespace {
 
+const char* const kStageNames[ARIEL_STAGE_COUNT] = {
+    "begin", "sort", "density", "forces", "p2g", "classify", "boundary_div", "solve", "gradient", "extrapolate",
+    "g2p_advect", "resample"};
+
 ariel_status enqueue_stage(ariel_sim* s, int g, cudaEvent_t* evs = nullptr) {
+    NvtxRange range(g >= 0 && g < ARIEL_STAGE_COUNT ? kStageNames[g] : "stage");
     const DevState& S = s->S;
     cudaStream_t st = s->stream;
     cudaError_t e = cudaSuccess;
@@ -1076,6 +1081,7 @@ ariel_status ariel_scene_count(ariel_sim* s, int32_t* k) {
 
 ariel_status ariel_init(ariel_sim* s) {
     if (!s) return ARIEL_ERR_INVALID_ARG;
+    NvtxRange range("ariel_init");
     // m_max_density from the 10^3 lattice, per scene (flip.cpp:47-70)
     ARIEL_TRY(compute_max_density(s));
     for (int i = 0; i < s->k; ++i) {
@@ -1149,6 +1155,7 @@ ariel_status ariel_stage(ariel_sim* s, int32_t stage) {
 ariel_status ariel_step(ariel_sim* s, int32_t nsteps) {
     if (!s || nsteps < 0) return ARIEL_ERR_INVALID_ARG;
     if (!s->inited) return ARIEL_ERR_STATE;
+    NvtxRange range("ariel_step");
     for (int it = 0; it < nsteps; ++it) {
         ARIEL_TRY(step_async(s));
         if (s->prm.fail_on_not_converged) {

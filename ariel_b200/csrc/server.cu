@@ -184,6 +184,7 @@ void prepare_main(ariel_server* S) {
             S->preparing++;
         }
         HostParticles hp;
+        NvtxRange range("server_seed");
         generate_particles(r->desc, hp);
         const long long np = (long long)hp.pos4.size(), ns = (long long)hp.solid_pos.size();
         const long long bytes = state_bytes({r->desc}, {np}, {ns}, S->prm);
@@ -247,6 +248,7 @@ void fail_live(ariel_server* S, ariel_status st) {
 // `add` into a new batch.  Called by the worker with no step in flight.
 ariel_status relayout(ariel_server* S, const std::vector<Request*>& retire, const std::vector<Request*>& keep,
                       std::vector<Request*>& add) {
+    NvtxRange range("server_repack");
     const double t_begin = S->now_ms();
     ariel_sim* old = S->batch;
     if (old) {

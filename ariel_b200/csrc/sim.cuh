@@ -7,9 +7,17 @@
 #include <cstring>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "pcg.cuh"
 
 namespace ariel {
+
+// Named NVTX range for profilers (a no-op unless a tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 struct DeviceBuf {
     void* p = nullptr;
