@@ -22,7 +22,7 @@ import os
 from . import _abi as A
 
 BLOCKS_PER_SM = (1, 2)
-BRICKS = ((8, 16, 16), (16, 16, 8), (8, 8, 32), (12, 12, 12), (16, 8, 16), (4, 16, 32), (8, 8, 16))
+BRICKS = ((12, 12, 12), (8, 16, 16), (16, 16, 8), (8, 8, 32), (16, 8, 16), (6, 12, 24), (10, 10, 10), (8, 8, 16))
 
 
 def brick_ok(b):

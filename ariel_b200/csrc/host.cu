@@ -167,9 +167,10 @@ void sweep_brick(const AsimParams& p, int& bx, int& by, int& bz) {
     by = p.sweep_brick[1];
     bz = p.sweep_brick[2];
     if (bx == 0 && by == 0 && bz == 0) {
-        bx = 8;
-        by = 16;
-        bz = 16;
+        // fastest of the autotuner's candidates at 128^3 (MIC(0), MIXED)
+        bx = 12;
+        by = 12;
+        bz = 12;
     }
 }
 

@@ -161,7 +161,7 @@ typedef struct AsimParams {
                                    depend on it; tests and tuning); 0 = one grid of resident blocks */
     int32_t sweep_brick[3];     /* brick (i, j, k extents in cells) of the ordered wavefront sweeps
                                    (MIC(0) and the reference's PRef==1 path); results do not depend
-                                   on it.  0,0,0 = default 8,16,16.  Limits: i,j <= 31, k <= 63,
+                                   on it.  0,0,0 = default 12,12,12.  Limits: i,j <= 31, k <= 63,
                                    product <= 2048, (i+1)(j+1)(k+1) <= 2744 */
 } AsimParams;
 
