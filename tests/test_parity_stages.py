@@ -17,11 +17,20 @@ from oracle.pyoracle import RefSim
 
 from helpers import assert_bits, dambreak, evolved_state, params, stage_parity
 
+def _with_density(desc, density):
+    desc.density = density
+    return desc
+
+
 CASES = [
     ("dambreak16_fresh", dambreak(16, seed=3), 0),
     ("dambreak16_evolved", dambreak(16, seed=5), 6),
     ("dambreak20_sphere", dambreak(20, seed=7, hi=(0.35, 0.5, 1.0), spheres=[((0.6, 0.3, 0.5), 0.15)]), 4),
     ("dambreak24_evolved", dambreak(24, seed=11), 10),
+    # one particle per cell: resampling radius of a whole cell, no power-of-two shortcut
+    ("density1_n13", _with_density(dambreak(13, seed=13), 1.0), 3),
+    # 64 particles per cell: radii of a quarter cell
+    ("density025_n10", _with_density(dambreak(10, seed=17), 0.25), 2),
 ]
 
 
