@@ -182,7 +182,7 @@ int mode_of(const AsimParams& p) {
     return p.precision == ARIEL_PREC_FP64 ? kFp64 : (p.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
 }
 
-constexpr long long kChunkCells = 1024;  // the fast solve kernel's fixed chunk size
+constexpr long long kChunkCells = 2048;  // the fast solve kernel's fixed chunk size
 
 // The allocation list of build_state, in bytes (each buffer rounded to 256 bytes as the
 // allocators place them).  Kept next to build_state; a GPU test holds the two equal.
