@@ -746,7 +746,9 @@ cudaError_t launch_sort(const DevState& S, void* scan_tmp, cudaStream_t st) { re
 
 cudaError_t launch_density(const DevState& S, cudaStream_t st) {
     if (S.np == 0) return cudaSuccess;
-    k_density<<<grid_for(S.np), kBlock, 0, st>>>(S);
+    // 512 threads: measured faster than 256 for this kernel alone (0.79 vs 0.90 ms at 128^3)
+    constexpr int kDensityBlock = 512;
+    k_density<<<grid_for(S.np, kDensityBlock), kDensityBlock, 0, st>>>(S);
     count_launch();
     return cudaGetLastError();
 }
