@@ -182,8 +182,6 @@ int mode_of(const AsimParams& p) {
     return p.precision == ARIEL_PREC_FP64 ? kFp64 : (p.precision == ARIEL_PREC_MIXED ? kMixed : kRef32);
 }
 
-constexpr long long kChunkCells = 2048;  // the fast solve kernel's fixed chunk size
-
 // The allocation list of build_state, in bytes (each buffer rounded to 256 bytes as the
 // allocators place them).  Kept next to build_state; a GPU test holds the two equal.
 long long layout_bytes(const Layout& L) {
@@ -437,7 +435,7 @@ long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector
         L.nc += n * n * n;
         L.nf += 3 * n * n * (n + 1);
         L.ns += solids[i];
-        L.maxch += (n * n * n + kChunkCells - 1) / kChunkCells;
+        L.maxch += chunk_bound(n * n * n);
         if (descs[i].n_solid > 0) L.any_solid = true;
     }
     return layout_bytes(L);
@@ -482,7 +480,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
         s->sh[i].c_begin = s->cpref[i];
         s->sh[i].f_begin = s->fpref[i];
         if (s->descs[i].n_solid > 0) s->any_solid = true;
-        maxch += (n * n * n + kChunkCells - 1) / kChunkCells;
+        maxch += chunk_bound(n * n * n);
     }
     s->np = s->ppref[k];
     s->nc = s->cpref[k];
@@ -544,7 +542,6 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     A.stop_rule = s->prm.stop_rule;
     A.max_iters = s->prm.max_iters;
     A.max_outer = s->prm.max_outer > 0 ? s->prm.max_outer : 8;
-    A.chunk = (int)kChunkCells;
     A.fast = (k <= 128 && A.precond == ARIEL_PRECOND_REF) ? 1 : 0;
     // the reference preconditioner needs the ordered kernel only in the rare PRef == 1 case,
     // which only the device knows; keep launching it (it returns at once when not needed)

@@ -276,9 +276,11 @@ __global__ void k_pcg_tables(PcgArgs A, const uint32_t* scan) {
     for (int s = 0; s < k; ++s) {
         chp[s] = acc;
         long long nf = flp[s + 1] - flp[s];
-        acc += (nf + A.chunk - 1) / A.chunk;
+        const int sh = chunk_shift(nf);
+        acc += (nf + (1ll << sh) - 1) >> sh;
         PcgScene& P = A.sc[s];
         P.nf = (int)nf;
+        P.cshift = sh;
         P.ordered = nf > 0 && (A.precond == ARIEL_PRECOND_MIC0 || P.ones > 0);
         any_ordered |= P.ordered;
     }
@@ -668,9 +670,11 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
     const DevState& S = A.S;
     const int k = S.k;
     __shared__ long long fl_s[kMaxScenes + 1], ch_s[kMaxScenes + 1];
+    __shared__ uint8_t csh_s[kMaxScenes];
     for (int i = threadIdx.x; i <= k; i += blockDim.x) {
         fl_s[i] = A.fl_pref[i];
         ch_s[i] = A.ch_pref[i];
+        if (i < k) csh_s[i] = (uint8_t)A.sc[i].cshift;
     }
     __syncthreads();
     const long long nch = ch_s[k];
@@ -694,8 +698,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
 
     auto chunk_range = [&](long long ch, int& s, long long& t0, long long& t1) {
         s = find_scene(ch_s, k, ch);
-        t0 = fl_s[s] + (ch - ch_s[s]) * A.chunk;
-        t1 = min(t0 + (long long)A.chunk, fl_s[s + 1]);
+        const int sh = csh_s[s];
+        t0 = fl_s[s] + ((ch - ch_s[s]) << sh);
+        t1 = min(t0 + (1ll << sh), fl_s[s + 1]);
     };
     auto write_part = [&](long long ch, double a, double b) {
         block_sum2(a, b);
@@ -1304,9 +1309,7 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
 // first chunks in shared memory for the whole solve.
 // ==========================================================================================
 constexpr int kFastMaxScenes = 128;
-// 2048-cell chunks: measured against 512, 1024 and 4096 at 128^3 and on the 64-scene batch,
-// the fewest partial sums per reduction that still keep every block busy at 128^3.
-constexpr int kChunkCells = 2048;
+constexpr int kChunkCells = 1 << kChunkMaxShift;  // the largest chunk (cache slot size)
 constexpr int kFlCacheChunks = 2;
 
 struct SceneLocal {
@@ -1437,6 +1440,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     const DevState& S = A.S;
     const int k = S.k;
     __shared__ long long fl_s[kFastMaxScenes + 1], ch_s[kFastMaxScenes + 1];
+    __shared__ int csh_s[kFastMaxScenes];
     __shared__ SceneLocal L[kFastMaxScenes];
     __shared__ int s_active;
     // per-solve caches of this block's first kFlCacheChunks chunks: FLUID cell index,
@@ -1453,6 +1457,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
         SceneLocal z{};
         z.nf = A.sc[i].nf;
         L[i] = z;
+        csh_s[i] = A.sc[i].cshift;
     }
     __syncthreads();
     const long long nch = ch_s[k];
@@ -1498,8 +1503,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
             return false;
         }
         s = find_scene(ch_s, k, ch);
-        t0 = fl_s[s] + (ch - ch_s[s]) * kChunkCells;
-        t1 = min(t0 + (long long)kChunkCells, fl_s[s + 1]);
+        const int sh = csh_s[s];
+        t0 = fl_s[s] + ((ch - ch_s[s]) << sh);
+        t1 = min(t0 + (1ll << sh), fl_s[s + 1]);
         return true;
     };
     for (int j = 0; j < kFlCacheChunks; ++j) {
