@@ -215,6 +215,21 @@ __global__ void k_sort_permute(DevState S) {
 // ------------------------------------------------------------------------------------------
 // FlipSim::ComputeDensity (flip.cpp:697-733): one thread per slot, 27-cell gather.
 // ------------------------------------------------------------------------------------------
+// weightsum over slots [a, b) in slot order, with the Smooth kernel's division either exact
+// (POW2: h^2 a power of two, so r2 / h^2 == r2 * inv_hh) or as written.
+template <bool POW2>
+__device__ __forceinline__ float density_run(const float4* __restrict__ sp, uint32_t a, uint32_t b, float px,
+                                             float py, float pz, float hk, float inv_hh, float weightsum) {
+#pragma unroll 4
+    for (uint32_t t = a; t < b; ++t) {
+        const float4 q = sp[t];
+        const float sqd = sqrlength(q.x, q.y, q.z, px, py, pz);
+        const float weight = q.w * (POW2 ? gmax(1.0f - sqd * inv_hh, 0.0f) : smooth_k(sqd, hk));
+        weightsum = weightsum + weight;
+    }
+    return weightsum;
+}
+
 __global__ void k_density(DevState S) {
     SCENE_PREFIX(S.p_pref);
     long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -236,12 +251,8 @@ __global__ void k_density(DevState S) {
             if (sy < 0 || sy > n - 1) continue;
             long long cb = D.c_begin + ((long long)sx * n + sy) * n;
             uint32_t a = S.start[cb + z0], b = S.start[cb + z1 + 1];
-            for (uint32_t t = a; t < b; ++t) {
-                float4 q = S.spos4[t];
-                float sqd = sqrlength(q.x, q.y, q.z, p.x, p.y, p.z);
-                float weight = q.w * smooth_fast(sqd, hk, D.dens_pow2, D.dens_inv_hh);
-                weightsum = weightsum + weight;
-            }
+            weightsum = D.dens_pow2 ? density_run<true>(S.spos4, a, b, p.x, p.y, p.z, hk, D.dens_inv_hh, weightsum)
+                                    : density_run<false>(S.spos4, a, b, p.x, p.y, p.z, hk, D.dens_inv_hh, weightsum);
         }
     }
     S.dens[s] = weightsum / D.max_density;
@@ -492,6 +503,23 @@ __device__ __forceinline__ void axis_cells(float x, int c, int n, float ch, floa
     hi = b;
 }
 
+// The slot range of column (sx, sy) over z cells [zl, zh], without the end cells whose box is
+// farther than sqrt(lim) from x in 3D (gxy: the column's squared x-y gap); empty (a == b) when
+// the whole column is.  Only cells at the ends of the range can drop out, since the gap grows
+// away from the point, so the remaining slots stay contiguous and in order.
+__device__ __forceinline__ void column_slots(const DevState& S, const SceneDev& D, int sx, int sy, int zl, int zh,
+                                             float z, float gxy, float ch, float lim, uint32_t& a, uint32_t& b) {
+    const int n = D.n;
+    a = b = 0;
+    if (gxy > lim) return;
+    while (zl <= zh && gxy + cell_gap2(z, zl, n, ch) > lim) ++zl;
+    while (zh >= zl && gxy + cell_gap2(z, zh, n, ch) > lim) --zh;
+    if (zl > zh) return;
+    const long long cb = D.c_begin + ((long long)sx * n + sy) * n;
+    a = S.start[cb + zl];
+    b = S.start[cb + zh + 1];
+}
+
 // The resampler runs as two kernels over the slots of its own Sort: springs (the target
 // position t), then the velocity at t and the acceptance.  In both, each thread walks those of
 // the reference's 27 neighbour cells that reach within the kernel radius (about half a cell,
@@ -545,15 +573,15 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
         }
     };
     int xl, xh, yl, yh, zl, zh;
+    // of the reference's 27 cells, only those within the candidate radius (5% margin over the
+    // test below, for the rounding of the cell boxes)
+    const float ch = 1.0f / maxd, lim = 1.05f * near2;
     {
         const float gx = gmax(0.0f, gmin(maxd, maxd * p4.x)), gy = gmax(0.0f, gmin(maxd, maxd * p4.y)),
                     gz = gmax(0.0f, gmin(maxd, maxd * p4.z));
         nb_range(gx, n, xl, xh);
         nb_range(gy, n, yl, yh);
         nb_range(gz, n, zl, zh);
-        // of the reference's 27 cells, only those within the candidate radius (5% margin
-        // over the test below, for the rounding of the cell boxes)
-        const float ch = 1.0f / maxd, lim = 1.05f * near2;
         axis_cells(p4.x, min((int)gx, n - 1), n, ch, lim, xl, xh);
         axis_cells(p4.y, min((int)gy, n - 1), n, ch, lim, yl, yh);
         axis_cells(p4.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
@@ -562,8 +590,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
             for (int sy = yl; sy <= yh; ++sy) {
-                const long long cb = D.c_begin + ((long long)sx * n + sy) * n;
-                const uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                uint32_t a, b;
+                column_slots(S, D, sx, sy, zl, zh, p4.z,
+                             cell_gap2(p4.x, sx, n, ch) + cell_gap2(p4.y, sy, n, ch), ch, lim, a, b);
                 for (uint32_t t = a; t < b; ++t) {
                     const float4 q = S.spos4[t];
                     const float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
@@ -616,13 +645,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
         wsum += w;
     };
     int xl, xh, yl, yh, zl, zh;
+    const float ch = 1.0f / maxd, lim = 1.05f * re2;
     {
         const float gx = gmax(0.0f, gmin(maxd - 1, maxd * t.x)), gy = gmax(0.0f, gmin(maxd - 1, maxd * t.y)),
                     gz = gmax(0.0f, gmin(maxd - 1, maxd * t.z));
         nb_range(gx, n, xl, xh);
         nb_range(gy, n, yl, yh);
         nb_range(gz, n, zl, zh);
-        const float ch = 1.0f / maxd, lim = 1.05f * re2;
         axis_cells(t.x, min((int)gx, n - 1), n, ch, lim, xl, xh);
         axis_cells(t.y, min((int)gy, n - 1), n, ch, lim, yl, yh);
         axis_cells(t.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
@@ -631,8 +660,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
             for (int sy = yl; sy <= yh; ++sy) {
-                const long long cb = D.c_begin + ((long long)sx * n + sy) * n;
-                const uint32_t a = S.start[cb + zl], b = S.start[cb + zh + 1];
+                uint32_t a, b;
+                column_slots(S, D, sx, sy, zl, zh, t.z,
+                             cell_gap2(t.x, sx, n, ch) + cell_gap2(t.y, sy, n, ch), ch, lim, a, b);
                 for (uint32_t q = a; q < b; ++q) {
                     const float4 np = S.spos4[q];
                     // Sharpen is exactly 0 for dist2 >= re^2
