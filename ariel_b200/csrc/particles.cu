@@ -548,8 +548,9 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
     const uint32_t gid = (uint32_t)(S.sid[s] - D.p_begin);
     uint32_t draws = 0;
     float3 spring = make_float3(0, 0, 0);
-    // particleresampler.inl:58-78 for one neighbour slot t
+    // particleresampler.inl:58-78 for one neighbour slot t (the particle itself is skipped)
     auto eval = [&](uint32_t t) {
+        if (t == (uint32_t)s) return;
         const float springforce = 50.0f;
         float4 q = S.spos4[t];
         float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
@@ -593,12 +594,18 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
                 uint32_t a, b;
                 column_slots(S, D, sx, sy, zl, zh, p4.z,
                              cell_gap2(p4.x, sx, n, ch) + cell_gap2(p4.y, sy, n, ch), ch, lim, a, b);
-                for (uint32_t t = a; t < b; ++t) {
-                    const float4 q = S.spos4[t];
-                    const float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
-                    if (!(gdot3(d, d) < near2) || t == (uint32_t)s) continue;
-                    lst[nl][me] = t;
-                    if (++nl == kResList) {
+                for (uint32_t t = a; t < b;) {
+                    // a run of at most the list's free room: the list cannot overflow inside it,
+                    // so each candidate is stored unconditionally and kept by advancing nl
+                    const uint32_t e = min(b, t + (uint32_t)(kResList - nl));
+#pragma unroll 4
+                    for (; t < e; ++t) {
+                        const float4 q = S.spos4[t];
+                        const float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
+                        lst[nl][me] = t;
+                        nl += gdot3(d, d) < near2 ? 1 : 0;
+                    }
+                    if (nl == kResList) {
                         for (int i = 0; i < nl; ++i) eval(lst[i][me]);
                         nl = 0;
                     }
@@ -663,12 +670,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
                 uint32_t a, b;
                 column_slots(S, D, sx, sy, zl, zh, t.z,
                              cell_gap2(t.x, sx, n, ch) + cell_gap2(t.y, sy, n, ch), ch, lim, a, b);
-                for (uint32_t q = a; q < b; ++q) {
-                    const float4 np = S.spos4[q];
-                    // Sharpen is exactly 0 for dist2 >= re^2
-                    if (!(sqrlength(t.x, t.y, t.z, np.x, np.y, np.z) < re2)) continue;
-                    lst[nl][me] = q;
-                    if (++nl == kResList) {
+                for (uint32_t q = a; q < b;) {
+                    // runs of at most the list's free room, as in k_resample_spring; Sharpen is
+                    // exactly 0 for dist2 >= re^2
+                    const uint32_t e = min(b, q + (uint32_t)(kResList - nl));
+#pragma unroll 4
+                    for (; q < e; ++q) {
+                        const float4 np = S.spos4[q];
+                        lst[nl][me] = q;
+                        nl += sqrlength(t.x, t.y, t.z, np.x, np.y, np.z) < re2 ? 1 : 0;
+                    }
+                    if (nl == kResList) {
                         for (int i = 0; i < nl; ++i) eval(lst[i][me]);
                         nl = 0;
                     }
