@@ -232,7 +232,7 @@ long long layout_bytes(const Layout& L) {
     add(nc, 4);      // pc32
     const long long vb = L.mode == kFp64 ? 8 : 4;
     for (int i = 0; i < 8; ++i) add(nc, vb);
-    for (int i = 0; i < 3; ++i) add(4 * nc, vb);
+    for (int i = 0; i < 3; ++i) add((i < 2 ? 4 : 2) * nc, vb);
     if (L.mode == kMixed) {
         add(nc, 8);
         add(nc, 4);
@@ -579,7 +579,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     A.u = v[6];
     A.p = v[7];
     char* w4[3];
-    for (int i = 0; i < 3; ++i) ARIEL_TRY(dalloc(s, &w4[i], 4 * vb * (size_t)nc));
+    for (int i = 0; i < 3; ++i) ARIEL_TRY(dalloc(s, &w4[i], (i < 2 ? 4 : 2) * vb * (size_t)nc));
     A.va0 = w4[0];
     A.va1 = w4[1];
     A.vb = w4[2];

@@ -1318,6 +1318,15 @@ struct SceneLocal {
     int iters, outer, done, inner_done, converged, nf;
 };
 
+// Asynchronous 16-byte global -> shared copies (L1 bypassed), completed per thread.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(__cvta_generic_to_global(gmem))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned ld_acquire_cnt(const unsigned* p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -1386,7 +1395,29 @@ __device__ __forceinline__ void scene_sum3(const double* p0, const double* p1, c
 // Packed per-cell state of the single-reduction path (T = float for MIXED, double for FP64):
 //   Av[parity][c] = (r_i, w_i, s_{i-1}, pc)  -- read at c and its six neighbours, so
 //                                              double-buffered by iteration parity;
-//   Bv[c]         = (u_i, p_{i-1}, x_i, -)   -- read and written only by c's owner.
+//   Bv[c]         = (p_{i-1}, x_i)           -- read and written only by c's owner.
+// u_i = M r_i is not stored: its owner recomputes it as (r_i * pc) * pc from Av, the same
+// expression on the same values as in the iteration that produced r_i, so the same bits.
+template <class T>
+struct V2;
+template <>
+struct V2<float> {
+    using type = float2;
+};
+template <>
+struct V2<double> {
+    using type = double2;
+};
+template <class T>
+__device__ __forceinline__ typename V2<T>::type mk2(T a, T b);
+template <>
+__device__ __forceinline__ float2 mk2<float>(float a, float b) {
+    return make_float2(a, b);
+}
+template <>
+__device__ __forceinline__ double2 mk2<double>(double a, double b) {
+    return make_double2(a, b);
+}
 template <class T>
 struct V4;
 template <>
@@ -1474,6 +1505,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     constexpr int kDefer = 16;
     constexpr int kWarps = kPcgThreads / 32;
     __shared__ double dsum[kDefer][3][kWarps];
+    // records of the next round of an uncached chunk, one slot per thread and ILP lane
+    constexpr int kIlp = MODE == kFp64 ? 1 : 2;
+    __shared__ uint4 recbuf[kIlp][kPcgThreads];
     int npend = 0, jpend0 = 0;
     auto flush = [&]() {
         if (npend == 0) return;
@@ -1585,7 +1619,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     auto precond = [&](long long c, T rv) -> T { return (rv * pcv[c]) * pcv[c]; };
     T4* const Av0 = (T4*)A.va0;
     T4* const Av1 = (T4*)A.va1;
-    T4* const Bv = (T4*)A.vb;
+    using T2 = typename V2<T>::type;
+    T2* const Bv = (T2*)A.vb;
 
     int outer = 0;
     while (true) {
@@ -1664,7 +1699,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
         if (MODE != kRef32) {
             // ---- single-reduction PCG (Chronopoulos & Gear, 1989), one barrier per
             // iteration.  Iteration i reads Av[i&1] = (r_i, w_i, s_{i-1}, pc) at c and its
-            // neighbours and Bv = (u_i, p_{i-1}, x_i) at c, and writes s_i = w_i + beta s_{i-1},
+            // neighbours and Bv = (p_{i-1}, x_i) at c, and writes s_i = w_i + beta s_{i-1},
             // p_i = u_i + beta p_{i-1}, x_{i+1} = x_i + alpha p_i, r_{i+1} = r_i - alpha s_i,
             // u_{i+1} = M r_{i+1} and w_{i+1} = A u_{i+1}; the neighbour values of u_{i+1} are
             // recomputed from the same old state, bit-identically to what their owners write.
@@ -1693,7 +1728,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         T wv = acc * scale;
                         T xv = MODE == kMixed ? (T)0 : S.P64[c];
                         st4(Av0 + c, mk4<T>(rv, wv, (T)0, pcc));
-                        st4(Bv + c, mk4<T>(uv, (T)0, xv, (T)0));
+                        Bv[c] = mk2<T>((T)0, xv);
                         g0 += (double)rv * (double)uv;
                         d0 += (double)wv * (double)uv;
                         q0 += (double)rv * (double)rv;
@@ -1725,31 +1760,53 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         const long long nn = (long long)D.n * D.n, n1 = D.n;
                         // kIlp list entries per thread at once (t, t + blockDim.x, ...): their
                         // loads overlap; the sums still accumulate in ascending t per thread.
-                        constexpr int kIlp = MODE == kFp64 ? 1 : 2;
                         const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
+                        // Chunks past the cached ones read their records from global memory:
+                        // each round's records are copied into this thread's slots one round
+                        // ahead, so a round waits for one memory latency instead of two.
+                        const bool pf = j >= kFlCacheChunks;
+                        auto prefetch = [&](long long tb) {
+#pragma unroll
+                            for (int u = 0; u < kIlp; ++u) {
+                                const long long t = tb + (long long)u * blockDim.x;
+                                if (t < t1) cp_async16(&recbuf[u][threadIdx.x], A.rec + t);
+                            }
+                            cp_async_commit();
+                        };
+                        if (pf) prefetch(t0 + threadIdx.x);
                         for (long long tb = t0 + threadIdx.x; tb < t1; tb += (long long)kIlp * blockDim.x) {
                             long long c[kIlp];
                             uint32_t m[kIlp];
                             T dg[kIlp];
                             bool on[kIlp];
+                            if (pf) cp_async_wait_all();
 #pragma unroll
                             for (int u = 0; u < kIlp; ++u) {
                                 const long long t = tb + (long long)u * blockDim.x;
                                 on[u] = t < t1;
                                 if (on[u]) {
-                                    cell_rec(j, t, t0, c[u], m[u], dg[u]);
+                                    if (pf) {
+                                        const uint4 rc = recbuf[u][threadIdx.x];
+                                        c[u] = (long long)rc.x;
+                                        m[u] = rc.y;
+                                        dec_diag(rc, dg[u]);
+                                    } else {
+                                        cell_rec(j, t, t0, c[u], m[u], dg[u]);
+                                    }
                                 } else {
                                     c[u] = c[0];
                                     m[u] = 0u;
                                     dg[u] = (T)0;
                                 }
                             }
+                            if (pf) prefetch(tb + (long long)kIlp * blockDim.x);
                             // all loads first: own state and the six neighbours' (r, w, s, pc)
-                            T4 a[kIlp], b[kIlp], nb[kIlp][6];
+                            T4 a[kIlp], nb[kIlp][6];
+                            T2 b[kIlp];
 #pragma unroll
                             for (int u = 0; u < kIlp; ++u) {
                                 a[u] = ld4(Ac + c[u]);
-                                b[u] = ld4(Bv + c[u]);
+                                b[u] = Bv[c[u]];
 #pragma unroll
                                 for (int d = 0; d < 6; ++d)
                                     nb[u][d] = ld4(Ac + ((m[u] >> d) & 1u ? c[u] + off[d] : c[u]));
@@ -1758,8 +1815,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                             for (int u = 0; u < kIlp; ++u) {
                                 if (!on[u]) continue;
                                 const T sv = it == 0 ? a[u].y : a[u].y + bt * a[u].z;
-                                const T pvv = it == 0 ? b[u].x : b[u].x + bt * b[u].y;
-                                const T xv = b[u].z + al * pvv;
+                                const T ui = (a[u].x * a[u].w) * a[u].w;
+                                const T pvv = it == 0 ? ui : ui + bt * b[u].x;
+                                const T xv = b[u].y + al * pvv;
                                 const T rn = a[u].x - al * sv;
                                 const T un = (rn * a[u].w) * a[u].w;
                                 T acc = dg[u] * un;
@@ -1774,7 +1832,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                                 }
                                 const T wn = acc * scale;
                                 st4(An + c[u], mk4<T>(rn, wn, sv, a[u].w));
-                                st4(Bv + c[u], mk4<T>(un, pvv, xv, (T)0));
+                                Bv[c[u]] = mk2<T>(pvv, xv);
                                 g1 += (double)rn * (double)un;
                                 d1 += (double)wn * (double)un;
                                 q1 += (double)rn * (double)rn;
@@ -1816,8 +1874,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                 if (MODE == kMixed && L[s].done) continue;
                 for (long long t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
                     long long c = cell_at(j, t, t0);
-                    const T4 b = ld4(Bv + c);
-                    S.P64[c] = MODE == kMixed ? S.P64[c] + (double)b.z : (double)b.z;
+                    const T2 b = Bv[c];
+                    S.P64[c] = MODE == kMixed ? S.P64[c] + (double)b.y : (double)b.y;
                 }
             }
             if (MODE != kMixed) break;

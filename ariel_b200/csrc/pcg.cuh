@@ -86,7 +86,7 @@ struct PcgArgs {
     void* p;         // single-reduction PCG: search direction
     void* va0;       // fast single-reduction PCG: packed (r, w, s, pc), two parities
     void* va1;
-    void* vb;        // fast single-reduction PCG: packed (u, p, x, -)
+    void* vb;        // fast single-reduction PCG: packed (p, x)
     double* r64;     // MIXED outer residual
     float* d32;      // MIXED inner correction
     double* partial; // 3 * max chunks (three dot products per reduction)
