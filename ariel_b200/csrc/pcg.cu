@@ -1305,12 +1305,16 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
 // reaches e * gridDim.x), after which every block reads all chunk partials and reduces each
 // scene's range in the same fixed tree.  Every block therefore holds bit-identical copies of
 // every scene's alpha/beta/stop state in shared memory, and a barrier costs one arrival plus
-// one partial read on the critical path.  Each block also keeps the FLUID-cell indices of its
-// first chunks in shared memory for the whole solve.
+// one partial read on the critical path.  Each block also keeps the FLUID-list records of its
+// first chunk in shared memory for the whole solve and streams the others' through per-thread
+// prefetch slots.
 // ==========================================================================================
 constexpr int kFastMaxScenes = 128;
 constexpr int kChunkCells = 1 << kChunkMaxShift;  // the largest chunk (cache slot size)
-constexpr int kFlCacheChunks = 2;
+// Records of each block's first chunk stay in shared memory for the whole solve (at 128^3 that
+// is every chunk); later chunks stream theirs through the prefetch slots.  A second cached chunk
+// measured slower: the shared memory it takes comes out of the L1 the neighbour loads hit.
+constexpr int kFlCacheChunks = 1;
 
 struct SceneLocal {
     double bb, rr, rho, alpha, beta, target, rr_out;
@@ -1324,6 +1328,18 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(__cvta_generic_to_global(gmem))
                  : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(__cvta_generic_to_global(gmem))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_el(float4* smem, const float4* gmem) { cp_async16(smem, gmem); }
+__device__ __forceinline__ void cp_async_el(double4* smem, const double4* gmem) {
+    cp_async16(smem, gmem);
+    cp_async16(reinterpret_cast<char*>(smem) + 16, reinterpret_cast<const char*>(gmem) + 16);
+}
+__device__ __forceinline__ void cp_async_el(float2* smem, const float2* gmem) { cp_async8(smem, gmem); }
+__device__ __forceinline__ void cp_async_el(double2* smem, const double2* gmem) { cp_async16(smem, gmem); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -1457,11 +1473,19 @@ __device__ __forceinline__ void dec_diag(const uint4& r, double& d) {
 }
 
 // Dynamic shared memory of k_pcg_fast: the per-solve caches of the block's first chunks
-// (diagonal, cell index, mask).
-size_t fast_dyn_smem(int mode) {
+// (diagonal, cell index, mask), then the single-reduction path's per-thread prefetch slots,
+// [kIlp][threads] each: records for 3 rounds, packed Av and packed Bv for 2 rounds.
+__host__ __device__ constexpr int fast_ilp(int mode) { return mode == kFp64 ? 1 : 2; }
+size_t fast_slot_bytes(int mode) {
+    if (mode == kRef32) return 0;
+    const size_t tb = mode == kFp64 ? 8 : 4;
+    return (size_t)2 * fast_ilp(mode) * kPcgThreads * (16 + 4 * tb + 2 * tb);
+}
+size_t fast_cache_bytes(int mode) {
     const size_t tb = mode == kFp64 ? 8 : 4;
     return (size_t)kFlCacheChunks * kChunkCells * (4 + 1 + tb);
 }
+size_t fast_dyn_smem(int mode) { return fast_cache_bytes(mode) + fast_slot_bytes(mode); }
 
 template <int MODE>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
@@ -1480,6 +1504,14 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     T* dgc = reinterpret_cast<T*>(dyn);
     uint32_t* flc = reinterpret_cast<uint32_t*>(dyn + sizeof(T) * kFlCacheChunks * kChunkCells);
     uint8_t* mkc = reinterpret_cast<uint8_t*>(flc + kFlCacheChunks * kChunkCells);
+    // prefetch slots of the single-reduction path, [buffer][ILP lane][thread]: records in 3
+    // buffers (round mod 3), own state in 2 (round parity)
+    using T2 = typename V2<T>::type;
+    constexpr int kIlp = fast_ilp(MODE);
+    uint4* const recbuf = reinterpret_cast<uint4*>(dyn + (size_t)kFlCacheChunks * kChunkCells * (sizeof(T) + 5));
+    T4* const ownA = reinterpret_cast<T4*>(recbuf + 2 * kIlp * kPcgThreads);
+    T2* const ownB = reinterpret_cast<T2*>(ownA + 2 * kIlp * kPcgThreads);
+    auto slot = [&](int buf, int u) { return (buf * kIlp + u) * kPcgThreads + (int)threadIdx.x; };
     for (int i = threadIdx.x; i <= k; i += blockDim.x) {
         fl_s[i] = A.fl_pref[i];
         ch_s[i] = A.ch_pref[i];
@@ -1505,9 +1537,6 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     constexpr int kDefer = 16;
     constexpr int kWarps = kPcgThreads / 32;
     __shared__ double dsum[kDefer][3][kWarps];
-    // records of the next round of an uncached chunk, one slot per thread and ILP lane
-    constexpr int kIlp = MODE == kFp64 ? 1 : 2;
-    __shared__ uint4 recbuf[kIlp][kPcgThreads];
     int npend = 0, jpend0 = 0;
     auto flush = [&]() {
         if (npend == 0) return;
@@ -1619,7 +1648,6 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     auto precond = [&](long long c, T rv) -> T { return (rv * pcv[c]) * pcv[c]; };
     T4* const Av0 = (T4*)A.va0;
     T4* const Av1 = (T4*)A.va1;
-    using T2 = typename V2<T>::type;
     T2* const Bv = (T2*)A.vb;
 
     int outer = 0;
@@ -1761,56 +1789,17 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         // kIlp list entries per thread at once (t, t + blockDim.x, ...): their
                         // loads overlap; the sums still accumulate in ascending t per thread.
                         const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
-                        // Chunks past the cached ones read their records from global memory:
-                        // each round's records are copied into this thread's slots one round
-                        // ahead, so a round waits for one memory latency instead of two.
-                        const bool pf = j >= kFlCacheChunks;
-                        auto prefetch = [&](long long tb) {
+                        const long long step = (long long)kIlp * blockDim.x;
+                        // One round: the six neighbours' (r, w, s, pc), then the update of the
+                        // round's cells from their own state (a, b).
+                        auto round = [&](const long long* c, const uint32_t* m, const T* dg, const bool* on,
+                                         const T4* a, const T2* b) {
+                            T4 nb[kIlp][6];
 #pragma unroll
-                            for (int u = 0; u < kIlp; ++u) {
-                                const long long t = tb + (long long)u * blockDim.x;
-                                if (t < t1) cp_async16(&recbuf[u][threadIdx.x], A.rec + t);
-                            }
-                            cp_async_commit();
-                        };
-                        if (pf) prefetch(t0 + threadIdx.x);
-                        for (long long tb = t0 + threadIdx.x; tb < t1; tb += (long long)kIlp * blockDim.x) {
-                            long long c[kIlp];
-                            uint32_t m[kIlp];
-                            T dg[kIlp];
-                            bool on[kIlp];
-                            if (pf) cp_async_wait_all();
-#pragma unroll
-                            for (int u = 0; u < kIlp; ++u) {
-                                const long long t = tb + (long long)u * blockDim.x;
-                                on[u] = t < t1;
-                                if (on[u]) {
-                                    if (pf) {
-                                        const uint4 rc = recbuf[u][threadIdx.x];
-                                        c[u] = (long long)rc.x;
-                                        m[u] = rc.y;
-                                        dec_diag(rc, dg[u]);
-                                    } else {
-                                        cell_rec(j, t, t0, c[u], m[u], dg[u]);
-                                    }
-                                } else {
-                                    c[u] = c[0];
-                                    m[u] = 0u;
-                                    dg[u] = (T)0;
-                                }
-                            }
-                            if (pf) prefetch(tb + (long long)kIlp * blockDim.x);
-                            // all loads first: own state and the six neighbours' (r, w, s, pc)
-                            T4 a[kIlp], nb[kIlp][6];
-                            T2 b[kIlp];
-#pragma unroll
-                            for (int u = 0; u < kIlp; ++u) {
-                                a[u] = ld4(Ac + c[u]);
-                                b[u] = Bv[c[u]];
+                            for (int u = 0; u < kIlp; ++u)
 #pragma unroll
                                 for (int d = 0; d < 6; ++d)
                                     nb[u][d] = ld4(Ac + ((m[u] >> d) & 1u ? c[u] + off[d] : c[u]));
-                            }
 #pragma unroll
                             for (int u = 0; u < kIlp; ++u) {
                                 if (!on[u]) continue;
@@ -1836,6 +1825,113 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                                 g1 += (double)rn * (double)un;
                                 d1 += (double)wn * (double)un;
                                 q1 += (double)rn * (double)rn;
+                            }
+                        };
+                        if (j >= kFlCacheChunks) {
+                            // Records and own state of chunks past the cached ones come from
+                            // global memory: both are copied into this thread's slots ahead of
+                            // use (own state one round, records two), and no copy targets a slot
+                            // read in the same round, so a round waits only for its neighbours.
+                            auto issue_rec = [&](long long tb, int par) {
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u) {
+                                    const long long t = tb + (long long)u * blockDim.x;
+                                    if (t < t1) cp_async16(recbuf + slot(par, u), A.rec + t);
+                                }
+                            };
+                            auto read_rec = [&](long long tb, int par, long long* c, uint32_t* m, T* dg, bool* on) {
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u) {
+                                    const long long t = tb + (long long)u * blockDim.x;
+                                    on[u] = t < t1;
+                                    if (on[u]) {
+                                        const uint4 rc = recbuf[slot(par, u)];
+                                        c[u] = (long long)rc.x;
+                                        m[u] = rc.y;
+                                        dec_diag(rc, dg[u]);
+                                    } else {
+                                        c[u] = c[0];
+                                        m[u] = 0u;
+                                        dg[u] = (T)0;
+                                    }
+                                }
+                            };
+                            auto issue_own = [&](const long long* c, const bool* on, int par) {
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u)
+                                    if (on[u]) {
+                                        cp_async_el(ownA + slot(par, u), Ac + c[u]);
+                                        cp_async_el(ownB + slot(par, u), Bv + c[u]);
+                                    }
+                            };
+                            long long c[kIlp], cn[kIlp];
+                            uint32_t m[kIlp], mn[kIlp];
+                            T dg[kIlp], dn[kIlp];
+                            bool on[kIlp], onn[kIlp];
+                            long long tb = t0 + threadIdx.x;
+                            if (tb < t1) {
+                                issue_rec(tb, 0);
+                                cp_async_commit();
+                                cp_async_wait_all();
+                                read_rec(tb, 0, c, m, dg, on);
+                                issue_own(c, on, 0);
+                                if (tb + step < t1) issue_rec(tb + step, 1);
+                                cp_async_commit();
+                            }
+                            for (int r = 0; tb < t1; tb += step, ++r) {
+                                const int cur = r & 1, nxt = cur ^ 1;
+                                cp_async_wait_all();  // own state of this round, records of the next
+                                T4 a[kIlp];
+                                T2 b[kIlp];
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u) {
+                                    a[u] = ld4(ownA + slot(cur, u));
+                                    b[u] = ownB[slot(cur, u)];
+                                }
+                                const bool more = tb + step < t1;
+                                if (more) {
+                                    read_rec(tb + step, nxt, cn, mn, dn, onn);
+                                    issue_own(cn, onn, nxt);
+                                    if (tb + 2 * step < t1) issue_rec(tb + 2 * step, cur);
+                                }
+                                cp_async_commit();
+                                round(c, m, dg, on, a, b);
+                                if (more) {
+#pragma unroll
+                                    for (int u = 0; u < kIlp; ++u) {
+                                        c[u] = cn[u];
+                                        m[u] = mn[u];
+                                        dg[u] = dn[u];
+                                        on[u] = onn[u];
+                                    }
+                                }
+                            }
+                        } else {
+                            for (long long tb = t0 + threadIdx.x; tb < t1; tb += step) {
+                                long long c[kIlp];
+                                uint32_t m[kIlp];
+                                T dg[kIlp];
+                                bool on[kIlp];
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u) {
+                                    const long long t = tb + (long long)u * blockDim.x;
+                                    on[u] = t < t1;
+                                    if (on[u]) {
+                                        cell_rec(j, t, t0, c[u], m[u], dg[u]);
+                                    } else {
+                                        c[u] = c[0];
+                                        m[u] = 0u;
+                                        dg[u] = (T)0;
+                                    }
+                                }
+                                T4 a[kIlp];
+                                T2 b[kIlp];
+#pragma unroll
+                                for (int u = 0; u < kIlp; ++u) {
+                                    a[u] = ld4(Ac + c[u]);
+                                    b[u] = Bv[c[u]];
+                                }
+                                round(c, m, dg, on, a, b);
                             }
                         }
                     }

@@ -163,7 +163,7 @@ def test_solve_independent_of_grid_size(precision):
     packed per-entry records) gives the same bits as the default grid: every chunk's partial
     sums and the tree over chunks are fixed by the FLUID list alone."""
     desc, st, g = _solve_inputs(32)
-    assert (g["A"] == A.FLUID).sum() > 4096  # 9+ chunks of 512 cells, more than one block caches (two)
+    assert (g["A"] == A.FLUID).sum() > 4096  # 9+ chunks of 512 cells: one cached per block, the rest streamed
     runs = [_gpu_solve(desc, st, g, params(precision=precision, stop=A.STOP_REL, tol=1e-6, pcg_grid_blocks=nb))
             for nb in (0, 1)]
     for key in ("P", "P64"):
