@@ -1479,7 +1479,7 @@ __host__ __device__ constexpr int fast_ilp(int mode) { return mode == kFp64 ? 1 
 size_t fast_slot_bytes(int mode) {
     if (mode == kRef32) return 0;
     const size_t tb = mode == kFp64 ? 8 : 4;
-    return (size_t)2 * fast_ilp(mode) * kPcgThreads * (16 + 4 * tb + 2 * tb);
+    return (size_t)fast_ilp(mode) * kPcgThreads * (3 * 16 + 2 * (4 * tb + 2 * tb));
 }
 size_t fast_cache_bytes(int mode) {
     const size_t tb = mode == kFp64 ? 8 : 4;
@@ -1509,7 +1509,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     using T2 = typename V2<T>::type;
     constexpr int kIlp = fast_ilp(MODE);
     uint4* const recbuf = reinterpret_cast<uint4*>(dyn + (size_t)kFlCacheChunks * kChunkCells * (sizeof(T) + 5));
-    T4* const ownA = reinterpret_cast<T4*>(recbuf + 2 * kIlp * kPcgThreads);
+    T4* const ownA = reinterpret_cast<T4*>(recbuf + 3 * kIlp * kPcgThreads);
     T2* const ownB = reinterpret_cast<T2*>(ownA + 2 * kIlp * kPcgThreads);
     auto slot = [&](int buf, int u) { return (buf * kIlp + u) * kPcgThreads + (int)threadIdx.x; };
     for (int i = threadIdx.x; i <= k; i += blockDim.x) {
@@ -1775,6 +1775,87 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
             for (int it = 0;; ++it) {
                 const T4* Ac = (it & 1) ? Av1 : Av0;
                 T4* An = (it & 1) ? Av0 : Av1;
+                const int step = kIlp * (int)blockDim.x;
+                // This thread's rounds in the streamed chunks (those past the cached ones) form one
+                // pipeline across chunk boundaries: a round's records and own state are copied
+                // into this thread's slots ahead of use (own state one round, records two), and no
+                // copy targets a slot read in the same round, so a round waits only for its
+                // neighbours' loads.  A position is (chunk j, chunk end t1, round start tb); list
+                // indices fit 32 bits (fewer than 2^31 cells).
+                struct Pos {
+                    int j, t1, tb;
+                };
+                // to this thread's next round in an active streamed chunk; false past the last
+                auto advance = [&](Pos& p) -> bool {
+                    if (p.tb + step < p.t1) {
+                        p.tb += step;
+                        return true;
+                    }
+                    for (int jj = p.j + 1;; ++jj) {
+                        const long long ch = blockIdx.x + (long long)jj * gridDim.x;
+                        if (ch >= nch) return false;
+                        const int s2 = find_scene(ch_s, k, ch);
+                        const int sh = csh_s[s2];
+                        const long long a0 = fl_s[s2] + ((ch - ch_s[s2]) << sh);
+                        const long long a1 = min(a0 + (1ll << sh), fl_s[s2 + 1]);
+                        if (L[s2].inner_done || a0 + (long long)threadIdx.x >= a1) continue;
+                        p.j = jj;
+                        p.t1 = (int)a1;
+                        p.tb = (int)a0 + (int)threadIdx.x;
+                        return true;
+                    }
+                };
+                auto issue_rec = [&](const Pos& p, int par) {
+#pragma unroll
+                    for (int u = 0; u < kIlp; ++u) {
+                        const int t = p.tb + u * (int)blockDim.x;
+                        if (t < p.t1) cp_async16(recbuf + slot(par, u), A.rec + t);
+                    }
+                };
+                auto read_rec = [&](const Pos& p, int par, long long* c, uint32_t* m, T* dg, bool* on) {
+#pragma unroll
+                    for (int u = 0; u < kIlp; ++u) {
+                        on[u] = p.tb + u * (int)blockDim.x < p.t1;
+                        if (on[u]) {
+                            const uint4 rc = recbuf[slot(par, u)];
+                            c[u] = (long long)rc.x;
+                            m[u] = rc.y;
+                            dec_diag(rc, dg[u]);
+                        } else {
+                            c[u] = c[0];
+                            m[u] = 0u;
+                            dg[u] = (T)0;
+                        }
+                    }
+                };
+                auto issue_own = [&](const long long* c, const bool* on, int par) {
+#pragma unroll
+                    for (int u = 0; u < kIlp; ++u)
+                        if (on[u]) {
+                            cp_async_el(ownA + slot(par, u), Ac + c[u]);
+                            cp_async_el(ownB + slot(par, u), Bv + c[u]);
+                        }
+                };
+                // pipeline state: the current position p0 and the next p1; round R keeps its
+                // records in buffer R mod 3 (rb) and its own state in buffer R mod 2
+                Pos p0{kFlCacheChunks - 1, 0, 0}, p1{0, 0, 0};
+                bool v0 = advance(p0), v1 = false;
+                int R = 0, rb = 0;
+                if (v0) {
+                    issue_rec(p0, 0);
+                    cp_async_commit();
+                    cp_async_wait_all();
+                    long long c[kIlp];
+                    uint32_t m[kIlp];
+                    T dg[kIlp];
+                    bool on[kIlp];
+                    read_rec(p0, 0, c, m, dg, on);
+                    issue_own(c, on, 0);
+                    p1 = p0;
+                    v1 = advance(p1);
+                    if (v1) issue_rec(p1, 1);
+                    cp_async_commit();
+                }
                 for (int j = 0;; ++j) {
                     int s;
                     long long t0, t1;
@@ -1788,8 +1869,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         const long long nn = (long long)D.n * D.n, n1 = D.n;
                         // kIlp list entries per thread at once (t, t + blockDim.x, ...): their
                         // loads overlap; the sums still accumulate in ascending t per thread.
-                        const long long off[6] = {-nn, nn, -n1, n1, -1, 1};
-                        const long long step = (long long)kIlp * blockDim.x;
+                        auto off = [&](int d) -> long long {
+                            return d == 0 ? -nn : d == 1 ? nn : d == 2 ? -n1 : d == 3 ? n1 : d == 4 ? -1ll : 1ll;
+                        };
                         // One round: the six neighbours' (r, w, s, pc), then the update of the
                         // round's cells from their own state (a, b).
                         auto round = [&](const long long* c, const uint32_t* m, const T* dg, const bool* on,
@@ -1799,7 +1881,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                             for (int u = 0; u < kIlp; ++u)
 #pragma unroll
                                 for (int d = 0; d < 6; ++d)
-                                    nb[u][d] = ld4(Ac + ((m[u] >> d) & 1u ? c[u] + off[d] : c[u]));
+                                    nb[u][d] = ld4(Ac + ((m[u] >> d) & 1u ? c[u] + off(d) : c[u]));
 #pragma unroll
                             for (int u = 0; u < kIlp; ++u) {
                                 if (!on[u]) continue;
@@ -1828,83 +1910,41 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                             }
                         };
                         if (j >= kFlCacheChunks) {
-                            // Records and own state of chunks past the cached ones come from
-                            // global memory: both are copied into this thread's slots ahead of
-                            // use (own state one round, records two), and no copy targets a slot
-                            // read in the same round, so a round waits only for its neighbours.
-                            auto issue_rec = [&](long long tb, int par) {
-#pragma unroll
-                                for (int u = 0; u < kIlp; ++u) {
-                                    const long long t = tb + (long long)u * blockDim.x;
-                                    if (t < t1) cp_async16(recbuf + slot(par, u), A.rec + t);
-                                }
-                            };
-                            auto read_rec = [&](long long tb, int par, long long* c, uint32_t* m, T* dg, bool* on) {
-#pragma unroll
-                                for (int u = 0; u < kIlp; ++u) {
-                                    const long long t = tb + (long long)u * blockDim.x;
-                                    on[u] = t < t1;
-                                    if (on[u]) {
-                                        const uint4 rc = recbuf[slot(par, u)];
-                                        c[u] = (long long)rc.x;
-                                        m[u] = rc.y;
-                                        dec_diag(rc, dg[u]);
-                                    } else {
-                                        c[u] = c[0];
-                                        m[u] = 0u;
-                                        dg[u] = (T)0;
-                                    }
-                                }
-                            };
-                            auto issue_own = [&](const long long* c, const bool* on, int par) {
-#pragma unroll
-                                for (int u = 0; u < kIlp; ++u)
-                                    if (on[u]) {
-                                        cp_async_el(ownA + slot(par, u), Ac + c[u]);
-                                        cp_async_el(ownB + slot(par, u), Bv + c[u]);
-                                    }
-                            };
-                            long long c[kIlp], cn[kIlp];
-                            uint32_t m[kIlp], mn[kIlp];
-                            T dg[kIlp], dn[kIlp];
-                            bool on[kIlp], onn[kIlp];
-                            long long tb = t0 + threadIdx.x;
-                            if (tb < t1) {
-                                issue_rec(tb, 0);
-                                cp_async_commit();
-                                cp_async_wait_all();
-                                read_rec(tb, 0, c, m, dg, on);
-                                issue_own(c, on, 0);
-                                if (tb + step < t1) issue_rec(tb + step, 1);
-                                cp_async_commit();
-                            }
-                            for (int r = 0; tb < t1; tb += step, ++r) {
-                                const int cur = r & 1, nxt = cur ^ 1;
+                            while (v0 && p0.j == j) {
+                                const int rb1 = rb == 2 ? 0 : rb + 1, rb2 = rb1 == 2 ? 0 : rb1 + 1;
                                 cp_async_wait_all();  // own state of this round, records of the next
+                                Pos p2 = p1;
+                                bool v2 = false;
+                                if (v1) {
+                                    long long cn[kIlp];
+                                    uint32_t mn[kIlp];
+                                    T dn[kIlp];
+                                    bool onn[kIlp];
+                                    read_rec(p1, rb1, cn, mn, dn, onn);
+                                    issue_own(cn, onn, (R + 1) & 1);
+                                    v2 = advance(p2);
+                                    if (v2) issue_rec(p2, rb2);
+                                }
+                                cp_async_commit();
+                                long long c[kIlp];
+                                uint32_t m[kIlp];
+                                T dg[kIlp];
+                                bool on[kIlp];
+                                read_rec(p0, rb, c, m, dg, on);
                                 T4 a[kIlp];
                                 T2 b[kIlp];
 #pragma unroll
                                 for (int u = 0; u < kIlp; ++u) {
-                                    a[u] = ld4(ownA + slot(cur, u));
-                                    b[u] = ownB[slot(cur, u)];
+                                    a[u] = ld4(ownA + slot(R & 1, u));
+                                    b[u] = ownB[slot(R & 1, u)];
                                 }
-                                const bool more = tb + step < t1;
-                                if (more) {
-                                    read_rec(tb + step, nxt, cn, mn, dn, onn);
-                                    issue_own(cn, onn, nxt);
-                                    if (tb + 2 * step < t1) issue_rec(tb + 2 * step, cur);
-                                }
-                                cp_async_commit();
                                 round(c, m, dg, on, a, b);
-                                if (more) {
-#pragma unroll
-                                    for (int u = 0; u < kIlp; ++u) {
-                                        c[u] = cn[u];
-                                        m[u] = mn[u];
-                                        dg[u] = dn[u];
-                                        on[u] = onn[u];
-                                    }
-                                }
+                                p0 = p1;
+                                v0 = v1;
+                                p1 = p2;
+                                v1 = v2;
+                                ++R;
+                                rb = rb1;
                             }
                         } else {
                             for (long long tb = t0 + threadIdx.x; tb < t1; tb += step) {
