@@ -29,10 +29,16 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic bytes of the persistent pressure-solve kernel per FLUID cell (unique bytes each
-# phase must move; see the solve section of the design notes).
-PCG_BYTES_PER_CELL_ITER = {"fp64": 113.0, "mixed": 65.0, "ref32": 61.0}
-PCG_BYTES_PER_CELL_OUTER = {"fp64": 69.0 + 16.0, "mixed": 89.0, "ref32": 35.0}
+# Algorithmic bytes of the persistent pressure-solve kernel per FLUID cell: the unique bytes each
+# phase must move (a neighbour's value is its owner's bytes, counted once; the cell records of
+# the bench workloads' first chunks stay in shared memory).
+#   inner CG iteration (single-reduction path): read packed Av (r, w, s, pc) and packed Bv
+#   (p, x), write both: MIXED 16 + 8 + 16 + 8 = 48, FP64 32 + 16 + 32 + 16 = 96.
+#   refinement sweep: residual (read P64, D; write r: 8 + 4 + 8), setup (read r, pc; write Av,
+#   Bv) and fold (read Bv [, P64]; write P64): MIXED 20 + 36 + 24 = 80, FP64 20 + 64 + 24 = 108.
+#   REF32 (the reference's two-reduction PCG): 61 per iteration, 35 per solve.
+PCG_BYTES_PER_CELL_ITER = {"fp64": 96.0, "mixed": 48.0, "ref32": 61.0}
+PCG_BYTES_PER_CELL_OUTER = {"fp64": 108.0, "mixed": 80.0, "ref32": 35.0}
 STAGE_NAMES = ["begin", "sort", "density", "forces", "p2g", "classify", "boundary_div", "solve",
                "gradient", "extrapolate", "g2p_advect", "resample"]
 
@@ -489,15 +495,26 @@ def main():
                  tot.cell_outer * PCG_BYTES_PER_CELL_OUTER[key]) / max(tot.solves, 1)
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else None
-    workload_key = "pcg_%s_%d" % (args.precision, args.n)
+    # DRAM traffic per launch from a committed capture of this very workload, if there is one
+    if args.workload == "batch":
+        workload_key = "pcg_%s_batch%d" % (args.precision, args.scenes)
+    else:
+        workload_key = "pcg_%s_%s%d" % (args.precision, args.workload, args.n)
     traffic = load_traffic(workload_key)
+    # the solve's packed state (Av twice, Bv) of the FLUID cells fits the 126 MB L2 or not;
+    # FLUID cells of all scenes from the per-scene sweep totals (cell_outer = sum nf * sweeps)
+    fluid_cells = tot.cell_outer * b.k / max(tot.outer, 1)
+    in_l2 = fluid_cells * (2 * 4 + 2) * (8 if args.precision == "fp64" else 4) < 100e6
     roofline = {"kernel": "k_pcg<%s> (persistent pressure solve)" % args.precision, "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": solve_ms,
-                "note": "frac of %s HBM copy bandwidth; at this size the working set stays in L2, so "
-                        "DRAM traffic (ncu capture) is far below the algorithmic bytes" % peak_kind}
+                "note": "frac of %s HBM copy bandwidth; " % peak_kind +
+                        ("the solve's working set stays in L2 at this size, so DRAM traffic is far below "
+                         "the algorithmic bytes" if in_l2 else
+                         "the solve's working set exceeds L2: DRAM traffic includes the streamed "
+                         "16-byte cell records (about 16 B per FLUID cell per iteration)")}
 
     out = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
