@@ -169,7 +169,9 @@ __global__ void k_sort_scatter(DevState S) {
     S.sid[S.start[c] + S.off[g]] = (uint32_t)g;
 }
 
-// Restores ascending particle id inside each cell (the reference's append order).
+// Restores ascending particle id inside each cell (the reference's append order): cells of up
+// to kSortRegs particles are sorted in registers, larger ones in place.
+constexpr int kSortRegs = 16;
 __global__ void k_sort_cells(DevState S) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= S.nc) return;
@@ -177,6 +179,24 @@ __global__ void k_sort_cells(DevState S) {
     if (b - a < 2) return;
     uint32_t* seg = S.sid + a;
     uint32_t m = b - a;
+    if (m <= kSortRegs) {
+        uint32_t v[kSortRegs];
+#pragma unroll
+        for (int i = 0; i < kSortRegs; ++i) v[i] = i < (int)m ? seg[i] : 0xffffffffu;
+        // odd-even transposition sort of the fixed-size array (the padding sorts last)
+#pragma unroll
+        for (int r = 0; r < kSortRegs; ++r)
+#pragma unroll
+            for (int i = r & 1; i + 1 < kSortRegs; i += 2) {
+                const uint32_t lo = min(v[i], v[i + 1]), hi = max(v[i], v[i + 1]);
+                v[i] = lo;
+                v[i + 1] = hi;
+            }
+#pragma unroll
+        for (int i = 0; i < kSortRegs; ++i)
+            if (i < (int)m) seg[i] = v[i];
+        return;
+    }
     for (uint32_t i = 1; i < m; ++i) {
         uint32_t v = seg[i];
         uint32_t j = i;

@@ -174,6 +174,29 @@ def test_solve_independent_of_grid_size(precision):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_batch_solve_independent_of_grid_size(precision):
+    """A batch of uneven scenes solved by 1 or 3 blocks steps to the same bits as with the default
+    grid.  With so few blocks each block streams chunks of several scenes through one prefetch
+    pipeline, across scene boundaries and past scenes that finish their solve early."""
+    descs = [dambreak(20, seed=2), dambreak(12, seed=3), dambreak(28, seed=4, hi=(0.3, 0.5, 1.0))]
+    runs = []
+    for nb in (0, 1, 3):
+        b = Batch(descs, params(precision=precision, stop=A.STOP_REL, tol=1e-6, pcg_grid_blocks=nb))
+        b.init()
+        b.step(3)
+        runs.append(([b.get_particles(i) for i in range(len(descs))],
+                     [b.stats(i).pcg_iterations for i in range(len(descs))]))
+        b.close()
+    ref_parts, ref_iters = runs[0]
+    for parts, iters in runs[1:]:
+        assert iters == ref_iters
+        for i in range(len(descs)):
+            for key in ("pos", "vel"):
+                assert np.array_equal(parts[i][key].view(np.uint8), ref_parts[i][key].view(np.uint8)), (i, key)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
 def test_mic0_independent_of_brick_and_grid(precision):
     """The wavefront sweeps give the same bits for any brick shape and any number of blocks:
     each cell's update reads the same values in the same order, only the schedule changes."""
