@@ -548,7 +548,8 @@ __device__ __forceinline__ void column_slots(const DevState& S, const SceneDev& 
 // so usually 2 per axis), testing only distance, records the few candidates in ascending slot
 // order -- the reference's summation order -- and then evaluates them with the reference's
 // exact arithmetic.  Neighbours outside the radius contribute exactly nothing.
-__global__ void __launch_bounds__(kBlock, 4) k_resample_spring(DevState S) {
+// Five blocks per SM (51 registers, a 12-byte spill): 1-2% faster than four.
+__global__ void __launch_bounds__(kBlock, 5) k_resample_spring(DevState S) {
     SCENE_PREFIX(S.p_pref);
     __shared__ uint32_t lst[kResList][kBlock];
     const int me = threadIdx.x;
