@@ -55,7 +55,9 @@ def _awkward_particles(n, seed=4):
         for y in (0.0, 0.5, 1.0):
             for z in (0.0, 1.0, 0.25):
                 pts.append((x, y, z))
-    pts += [(0.5, 0.5, 0.5)] * 12            # coincident: the resampler's jitter branch
+    # coincident: the resampler's jitter branch; 23 particles in one cell also take the sort's
+    # path for cells of more than 16 particles
+    pts += [(0.5, 0.5, 0.5)] * 20
     pts += [(0.5 + 1e-7, 0.5, 0.5)] * 3
     blk = rng.uniform(0.05, 0.45, size=(400, 3))
     blk[:, 1] *= 0.5
