@@ -4,8 +4,8 @@
 // function and lines it restates.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
 // baseline load this file's library; the product never does.
 //
-// PARITY UNPINNED: the reference cannot be compiled here (glm, TBB, OpenVDB, jsoncpp, Partio,
-// GLFW are absent) and it ships no tests or golden vectors.
+// Pinned to the reference's own code compiled from its sources (oracle/ref_driver.cpp,
+// oracle/_ref/): tests/test_reference_pin.py holds this file bit-identical to it.
 //
 // Restatement rules:
 //  * float arithmetic in the reference's expression order, compiled with -ffp-contract=off so no

@@ -5,10 +5,13 @@
  * calls), used as the parity checker of the CUDA library and as the timed CPU baseline.
  * Nothing in the product links or calls this code.
  *
- * PARITY UNPINNED: the reference cannot be compiled in this environment (it needs glm, TBB,
- * OpenVDB, jsoncpp, Partio and GLFW, none of which is installed) and it ships no tests, golden
- * vectors or example scenes.  The restatement is pinned only by hand-derived known answers and
- * by a second, independent numpy restatement (tests/golden/).
+ * PINNED to the reference's own code: oracle/Makefile's `reference` target compiles the
+ * reference's FLIP step from its unmodified sources (src/sim/flip.cpp with the .inl files it
+ * includes, src/grid/particlegrid.cpp) against stand-in headers for the absent glm, TBB and
+ * OpenVDB (oracle/refshim/, oracle/ref_driver.cpp) into oracle/_ref/.  tests/test_reference_pin.py
+ * holds this restatement bit-identical to it, whole steps and stage by stage, in the reference's
+ * configuration (fp32 PCG, its preconditioner and absolute stop rule).  Analytic solid spheres
+ * stand in for the reference's mesh solids on both sides.
  *
  * The entry points mirror the product's C ABI (include/ariel.h) with the prefix ariel_ref_.
  */

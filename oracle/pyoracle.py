@@ -1,7 +1,7 @@
 """TEST INFRASTRUCTURE ONLY: ctypes loader of the CPU oracle (oracle/ariel_oracle.cpp).
 
 Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg -- never by the
-product package.  Parity unpinned (see ariel_oracle.h).
+product package.  Pinned to the reference's own code (see ariel_oracle.h).
 """
 import ctypes as C
 import os

@@ -1,0 +1,2 @@
+// TEST INFRASTRUCTURE ONLY: see tbb.h in this folder.
+#include "tbb.h"
