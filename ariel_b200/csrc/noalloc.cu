@@ -12,8 +12,12 @@
 // exits (about 5.2 MB).  All calls share it and it keeps the previous call's contents, so the
 // per-cell counters are cleared at the start of every call, and calls that may run at the
 // same time on the GPU (different streams, threads, or overlapping work) race on it.
-#include <mutex>
-
+//
+// Order inside a cell: particles arrive in a cell in atomic order, and each cell's ids are then
+// put in ascending order -- by one thread for cells of at most 32 particles, by a block in
+// shared memory (bitonic network) up to 4096, and above that by a block that ranks every id
+// against the whole cell (work quadratic in that cell's size; positions outside the unit cube
+// are clamped into the edge cells, which is how such cells arise).
 #include "state.cuh"
 
 namespace {
@@ -22,13 +26,15 @@ constexpr long long kNaMaxParticles = 1ll << 20;  // 1,048,576 particles
 constexpr long long kNaMaxCells = 1ll << 18;      // 262,144 cells (a 64^3 grid)
 constexpr long long kNaTileSums = kNaMaxCells / 4096 + 2;
 constexpr long long kNaWords = kNaMaxCells + kNaMaxParticles + kNaTileSums;
+constexpr int kNaSmallCell = 32;    // cells up to this size: one thread, insertion sort
+constexpr int kNaSharedCell = 4096; // cells up to this size: one block, bitonic sort in shared memory
+constexpr int kNaBigBlock = 256;
 
 // Scratch layout (uint32 words): per-cell counts | per-particle arrival offsets | scan tiles.
+// After the scan and the scatter the first two regions are free again: the counts region then
+// lists the cells too large for one thread, the offsets region is the large-cell sort's
+// buffer, and the first scan word counts the listed cells.
 static __device__ __align__(256) uint32_t g_na_scratch[kNaWords];
-
-// Device addresses of g_na_scratch, looked up once per device with that device current.
-std::mutex g_na_mutex;
-uint32_t* g_na_addr[64] = {nullptr};
 
 __global__ void k_na_key(const float* __restrict__ pos, long long n, int dim, uint32_t* __restrict__ cell,
                          uint32_t* __restrict__ counts, uint32_t* __restrict__ offsets) {
@@ -51,11 +57,17 @@ __global__ void k_na_scatter(long long n, const uint32_t* __restrict__ cell, con
     order[start[c] + offsets[i]] = (uint32_t)i;
 }
 
-// Ascending particle id inside each cell, the order ParticleGrid::Sort appends them.
-__global__ void k_na_cells(long long ncells, const uint32_t* __restrict__ start, uint32_t* __restrict__ order) {
+// Ascending particle id inside each cell, the order ParticleGrid::Sort appends them.  Cells of
+// more than kNaSmallCell particles are listed for k_na_cells_big.
+__global__ void k_na_cells_small(long long ncells, const uint32_t* __restrict__ start, uint32_t* __restrict__ order,
+                                 uint32_t* __restrict__ big_list, uint32_t* __restrict__ big_count) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     uint32_t a = start[c], b = start[c + 1];
+    if (b - a > (uint32_t)kNaSmallCell) {
+        big_list[atomicAdd(big_count, 1u)] = (uint32_t)c;
+        return;
+    }
     for (uint32_t i = a + 1; i < b; ++i) {
         uint32_t v = order[i];
         uint32_t j = i;
@@ -67,26 +79,69 @@ __global__ void k_na_cells(long long ncells, const uint32_t* __restrict__ start,
     }
 }
 
-// Finds this device's copy of the scratch array.  Host code only knows the array's host-side
-// stand-in symbol, which must never be handed to a kernel; the device address comes from
-// cudaGetSymbolAddress with the device current.
-ariel_status na_scratch(uint32_t** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-        cudaGetLastError();
-        return ARIEL_ERR_NO_DEVICE;
-    }
-    std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? ARIEL_ERR_NO_DEVICE : ARIEL_ERR_CUDA;
+// One block per listed cell (grid-stride over the list).  Up to kNaSharedCell ids: bitonic sort
+// of the cell padded to a power of two in shared memory.  Beyond: every id's rank is the number
+// of smaller ids in the cell (ids are distinct), written to `tmp` at that rank, then copied back.
+__global__ void __launch_bounds__(kNaBigBlock) k_na_cells_big(const uint32_t* __restrict__ start,
+                                                              uint32_t* __restrict__ order,
+                                                              const uint32_t* __restrict__ big_list,
+                                                              const uint32_t* __restrict__ big_count,
+                                                              uint32_t* __restrict__ tmp) {
+    __shared__ uint32_t sh[kNaSharedCell];
+    const uint32_t nbig = *big_count;
+    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+        const uint32_t c = big_list[bi];
+        const uint32_t a = start[c], m = start[c + 1] - a;
+        if (m <= (uint32_t)kNaSharedCell) {
+            uint32_t p2 = 1;
+            while (p2 < m) p2 <<= 1;
+            for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) sh[i] = i < m ? order[a + i] : 0xFFFFFFFFu;
+            __syncthreads();
+            for (uint32_t k = 2; k <= p2; k <<= 1) {
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t i = threadIdx.x; i < p2; i += blockDim.x) {
+                        uint32_t l = i ^ j;
+                        if (l > i) {
+                            uint32_t x = sh[i], y = sh[l];
+                            bool up = (i & k) == 0;
+                            if ((x > y) == up) {
+                                sh[i] = y;
+                                sh[l] = x;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) order[a + i] = sh[i];
+            __syncthreads();
+        } else {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t v = order[a + i];
+                uint32_t rank = 0;
+                for (uint32_t q = 0; q < m; ++q) rank += order[a + q] < v ? 1u : 0u;
+                tmp[a + rank] = v;
+            }
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) order[a + i] = tmp[a + i];
+            __syncthreads();
         }
-        g_na_addr[dev] = (uint32_t*)p;
     }
-    *out = g_na_addr[dev];
+}
+
+// This device's copy of the scratch array.  Host code only knows the array's host-side
+// stand-in symbol, which must never be handed to a kernel; the device address comes from
+// cudaGetSymbolAddress with the device current.  It is looked up on every call (a host-side
+// lookup once the module is loaded, no allocation), so it stays right if the caller resets the
+// device and the module is loaded again at another address.
+ariel_status na_scratch(uint32_t** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? ARIEL_ERR_NO_DEVICE : ARIEL_ERR_CUDA;
+    }
+    *out = (uint32_t*)p;
     return ARIEL_OK;
 }
 
@@ -117,8 +172,19 @@ extern "C" ariel_status ariel_sort_by_cell_noalloc(const float* pos, int64_t n, 
     if (ariel::launch_scan_u32(counts, cell_start, ncells, tiles, s) != cudaSuccess) return ARIEL_ERR_CUDA;
     if (n > 0) {
         k_na_scatter<<<ariel::grid_for(n), ariel::kBlock, 0, s>>>(n, particle_cell, offsets, cell_start, order);
-        k_na_cells<<<ariel::grid_for(ncells), ariel::kBlock, 0, s>>>(ncells, cell_start, order);
-        ariel::count_launch(2);
+        // the scan is done with its tiles: its first word counts the cells too large for one thread
+        uint32_t* big_count = tiles;
+        if (cudaMemsetAsync(big_count, 0, sizeof(uint32_t), s) != cudaSuccess) {
+            cudaGetLastError();
+            return ARIEL_ERR_CUDA;
+        }
+        k_na_cells_small<<<ariel::grid_for(ncells), ariel::kBlock, 0, s>>>(ncells, cell_start, order, counts,
+                                                                          big_count);
+        int sms = 148;
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        k_na_cells_big<<<(unsigned)(2 * sms), kNaBigBlock, 0, s>>>(cell_start, order, counts, big_count, offsets);
+        ariel::count_launch(3);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? ARIEL_OK : ARIEL_ERR_CUDA;

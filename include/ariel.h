@@ -286,17 +286,23 @@ const char* ariel_last_error(void);
  * callers that cannot call cudaMalloc once running -- real-time loops that must not stall on an
  * allocation, and hosts whose own allocator owns all device memory and only hands out its
  * buffers.  Same binning as ARIEL_STAGE_SORT: for `n` particles at device positions `pos`
- * (xyz-interleaved floats, unit cube) on a `dim`^3 grid it writes, into caller-provided device
+ * (xyz-interleaved floats in the unit cube; coordinates outside it are clamped into the edge
+ * cells, as ParticleGrid::Sort does) on a `dim`^3 grid it writes, into caller-provided device
  * memory, the cell of every particle (particle_cell[n]), the exclusive prefix of per-cell counts
  * (cell_start[dim^3 + 1]) and the particle ids grouped by cell, ascending inside a cell
  * (order[n]).  Work is queued on `stream` (a cudaStream_t; NULL for the default stream) and the
  * call returns without waiting.
  * Limits: n <= 1,048,576 and dim^3 <= 262,144 (a 64^3 grid); larger requests return
  * ARIEL_ERR_INVALID_ARG.  Temporaries live in one fixed array of about 5.2 MB inside the
- * library, held on every GPU that loads it until the process exits.  The first call on a device
- * looks up that array's device address, so make it before any stream capture on that device.
+ * library, held on every GPU that loads it until the process exits.  Under CUDA's default lazy
+ * module loading that array is allocated when the library's module first loads on a device,
+ * i.e. by the first call there: make one call on each device at start-up, before any stream
+ * capture and before the caller's allocator takes over the device's memory (or run with
+ * CUDA_MODULE_LOADING=EAGER).  The array's device address is looked up on every call, so the
+ * entry point keeps working after the caller resets the device.
  * Every call reuses the array (per-cell counters are cleared by each call): calls that may
- * overlap on the GPU race and must be serialised by the caller. */
+ * overlap on the GPU race and must be serialised by the caller.  Cost is linear in n except for
+ * cells of more than 4,096 particles, which are ordered in time quadratic in their size. */
 ariel_status ariel_sort_by_cell_noalloc(const float* pos, int64_t n, int32_t dim, uint32_t* particle_cell,
                                         uint32_t* cell_start, uint32_t* order, void* stream);
 

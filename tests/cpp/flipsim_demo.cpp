@@ -1,4 +1,4 @@
-// Host program of the kind INTEGRATION.md describes: drives the B200 FLIP step through the
+// Host program driving the B200 FLIP step through the
 // C++ FlipSim wrapper.  Exit codes: 0 ran on a GPU, 3 the library reported no sm_100 device.
 #include <cstdio>
 #include <cstdlib>
