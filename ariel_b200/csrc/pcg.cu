@@ -276,11 +276,11 @@ __global__ void k_pcg_tables(PcgArgs A, const uint32_t* scan) {
     for (int s = 0; s < k; ++s) {
         chp[s] = acc;
         long long nf = flp[s + 1] - flp[s];
-        const int sh = chunk_shift(nf);
-        acc += (nf + (1ll << sh) - 1) >> sh;
+        const int cs = chunk_size(nf);
+        acc += (nf + cs - 1) / cs;
         PcgScene& P = A.sc[s];
         P.nf = (int)nf;
-        P.cshift = sh;
+        P.csize = cs;
         P.ordered = nf > 0 && (A.precond == ARIEL_PRECOND_MIC0 || P.ones > 0);
         any_ordered |= P.ordered;
     }
@@ -670,11 +670,11 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
     const DevState& S = A.S;
     const int k = S.k;
     __shared__ long long fl_s[kMaxScenes + 1], ch_s[kMaxScenes + 1];
-    __shared__ uint8_t csh_s[kMaxScenes];
+    __shared__ uint16_t csz_s[kMaxScenes];
     for (int i = threadIdx.x; i <= k; i += blockDim.x) {
         fl_s[i] = A.fl_pref[i];
         ch_s[i] = A.ch_pref[i];
-        if (i < k) csh_s[i] = (uint8_t)A.sc[i].cshift;
+        if (i < k) csz_s[i] = (uint16_t)A.sc[i].csize;
     }
     __syncthreads();
     const long long nch = ch_s[k];
@@ -698,9 +698,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
 
     auto chunk_range = [&](long long ch, int& s, long long& t0, long long& t1) {
         s = find_scene(ch_s, k, ch);
-        const int sh = csh_s[s];
-        t0 = fl_s[s] + ((ch - ch_s[s]) << sh);
-        t1 = min(t0 + (1ll << sh), fl_s[s + 1]);
+        const long long cs = csz_s[s];
+        t0 = fl_s[s] + (ch - ch_s[s]) * cs;
+        t1 = min(t0 + cs, fl_s[s + 1]);
     };
     auto write_part = [&](long long ch, double a, double b) {
         block_sum2(a, b);
@@ -1310,7 +1310,7 @@ cudaError_t launch_pcg_prepare(const PcgArgs& A, uint32_t* pred, uint32_t* scan,
 // prefetch slots.
 // ==========================================================================================
 constexpr int kFastMaxScenes = 128;
-constexpr int kChunkCells = 1 << kChunkMaxShift;  // the largest chunk (cache slot size)
+constexpr int kChunkCells = kChunkMax;  // the largest chunk (cache slot size)
 // Records of each block's first chunk stay in shared memory for the whole solve (at 128^3 that
 // is every chunk); later chunks stream theirs through the prefetch slots.  A second cached chunk
 // measured slower: the shared memory it takes comes out of the L1 the neighbour loads hit.
@@ -1349,14 +1349,20 @@ __device__ __forceinline__ unsigned ld_acquire_cnt(const unsigned* p) {
     return v;
 }
 
-// Barrier number `epoch` (1, 2, ...) of this launch.  Same ordering argument as grid_barrier.
+// Barrier number `epoch` (1, 2, ...) of this launch.  The block's writes are ordered before its
+// arrival by __syncthreads and thread 0's release reduction (cumulative over what the block's
+// barrier made visible to it); thread 0's acquire load that sees the count complete, followed by
+// __syncthreads, orders every thread's later loads after all blocks' arrivals -- the pattern of
+// grid_barrier with the release and acquire carried by the counter operations themselves.
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 __device__ bool count_barrier(Barrier* bar, int* dev_error, unsigned epoch, unsigned long long timeout_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         s_ok = 1;
-        __threadfence();
-        atomicAdd(&bar->count, 1u);
+        red_release_add(&bar->count, 1u);
         const unsigned target = epoch * gridDim.x;
         const unsigned long long t0 = gtimer();
         while (ld_acquire_cnt(&bar->count) < target) {
@@ -1372,7 +1378,6 @@ __device__ bool count_barrier(Barrier* bar, int* dev_error, unsigned epoch, unsi
             }
             __nanosleep(16);
         }
-        __threadfence();
     }
     __syncthreads();
     return s_ok != 0;
@@ -1495,7 +1500,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
     const DevState& S = A.S;
     const int k = S.k;
     __shared__ long long fl_s[kFastMaxScenes + 1], ch_s[kFastMaxScenes + 1];
-    __shared__ int csh_s[kFastMaxScenes];
+    __shared__ int csz_s[kFastMaxScenes];
     __shared__ SceneLocal L[kFastMaxScenes];
     __shared__ int s_active;
     // per-solve caches of this block's first kFlCacheChunks chunks: FLUID cell index,
@@ -1520,7 +1525,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
         SceneLocal z{};
         z.nf = A.sc[i].nf;
         L[i] = z;
-        csh_s[i] = A.sc[i].cshift;
+        csz_s[i] = A.sc[i].csize;
     }
     __syncthreads();
     const long long nch = ch_s[k];
@@ -1566,9 +1571,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
             return false;
         }
         s = find_scene(ch_s, k, ch);
-        const int sh = csh_s[s];
-        t0 = fl_s[s] + ((ch - ch_s[s]) << sh);
-        t1 = min(t0 + (1ll << sh), fl_s[s + 1]);
+        const long long cs = csz_s[s];
+        t0 = fl_s[s] + (ch - ch_s[s]) * cs;
+        t1 = min(t0 + cs, fl_s[s + 1]);
         return true;
     };
     for (int j = 0; j < kFlCacheChunks; ++j) {
@@ -1795,9 +1800,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
                         const long long ch = blockIdx.x + (long long)jj * gridDim.x;
                         if (ch >= nch) return false;
                         const int s2 = find_scene(ch_s, k, ch);
-                        const int sh = csh_s[s2];
-                        const long long a0 = fl_s[s2] + ((ch - ch_s[s2]) << sh);
-                        const long long a1 = min(a0 + (1ll << sh), fl_s[s2 + 1]);
+                        const long long cs = csz_s[s2];
+                        const long long a0 = fl_s[s2] + (ch - ch_s[s2]) * cs;
+                        const long long a1 = min(a0 + cs, fl_s[s2 + 1]);
                         if (L[s2].inner_done || a0 + (long long)threadIdx.x >= a1) continue;
                         p.j = jj;
                         p.t1 = (int)a1;

@@ -26,7 +26,7 @@ struct PcgScene {
     int ordered;      // preconditioner needs the ordered (wavefront) path
     int ones;         // FLUID cells whose order-free REF preconditioner value is exactly 1
     int nf;           // FLUID cells
-    int cshift;       // log2 of this scene's chunk size (FLUID cells per chunk)
+    int csize;        // this scene's chunk size (FLUID cells per chunk)
     int pad;
 };
 static_assert(sizeof(PcgScene) % 16 == 0, "PcgScene is copied as 16-byte words");
@@ -115,25 +115,26 @@ cudaError_t launch_barrier_selftest(Barrier* bar, int* err, unsigned long long t
 
 constexpr int kPcgThreads = 256;
 // Chunks of the FLUID list, the unit of every reduction's partial sums.  Each scene's chunk size
-// is the smallest power of two in [2^kChunkMinShift, 2^kChunkMaxShift] that cuts its FLUID list
-// into at most kChunkTarget chunks: a small scene still spreads over about as many blocks as a
-// large one, and a large one keeps few partial sums per reduction.  The size depends on the
-// scene alone, so a scene's bits do not depend on the batch it is solved in or on the grid.
-// Measured: against fixed 2048-cell chunks, 64^3 solves 1.6x faster, 128^3 the same and the
-// 64-scene batch 2% slower (its small scenes add chunks); a 256-cell floor or a target of 512
-// lost more on the batch.
-constexpr int kChunkMinShift = 9;
-constexpr int kChunkMaxShift = 11;
-constexpr long long kChunkTarget = 256;
-__host__ __device__ inline int chunk_shift(long long nf) {
-    int sh = kChunkMinShift;
-    while (sh < kChunkMaxShift && ((nf + (1ll << sh) - 1) >> sh) > kChunkTarget) ++sh;
-    return sh;
+// is the FLUID count split kChunkTarget ways (the persistent solve's resident blocks on a B200: 2
+// per SM x 148 SMs), rounded up to a multiple of kChunkAlign and kept within [kChunkMin,
+// kChunkMax]: a large scene then gives every resident block one chunk and every SM about the same
+// number of cells (with power-of-two sizes a 128^3 dam break left 79 SMs with twice the cells of
+// the others), a small one still spreads over as many blocks as 512-cell chunks allow, and a huge
+// one keeps chunks that fit the shared-memory record cache.  The size depends on the scene alone,
+// so a scene's bits do not depend on the batch it is solved in or on the grid.
+constexpr int kChunkMin = 512;
+constexpr int kChunkMax = 2048;
+constexpr int kChunkAlign = 64;
+constexpr long long kChunkTarget = 296;
+__host__ __device__ inline int chunk_size(long long nf) {
+    long long c = (nf + kChunkTarget - 1) / kChunkTarget;
+    c = (c + kChunkAlign - 1) / kChunkAlign * kChunkAlign;
+    return (int)(c < kChunkMin ? kChunkMin : (c > kChunkMax ? kChunkMax : c));
 }
 // Most chunks a scene of `cells` cells can have (its FLUID count is at most `cells`).
 inline long long chunk_bound(long long cells) {
-    const long long lo = (cells + (1ll << kChunkMinShift) - 1) >> kChunkMinShift;
-    const long long hi = (cells + (1ll << kChunkMaxShift) - 1) >> kChunkMaxShift;
+    const long long lo = (cells + kChunkMin - 1) / kChunkMin;
+    const long long hi = (cells + kChunkMax - 1) / kChunkMax;
     return std::min(lo, std::max(kChunkTarget, hi));
 }
 constexpr int kBrickMaxCells = 2048;

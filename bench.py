@@ -11,11 +11,13 @@ refinement) to a 1e-5 relative residual.  One "step" is one full FLIP step.
 
 Our arm prints one JSON line: device throughput (`value`, inputs resident in HBM, CUDA events
 around exactly K graph-replayed steps, max over ranks), the same metric end to end through
-the C ABI with host buffers (`e2e`), per-stage device times, PCG ms/solve beside the plain
-FP64 GPU path, p50/p99 step latency, the solve kernel's roofline, clocks, and the CPU
-oracle's throughput on a bounded sample (`cpu_baseline`).  `--impl reference` times the CPU
-restatement of the reference step (the reference itself cannot be built here) on the same
-workload.  Multi-GPU runs are independent replicas (one scene per GPU, no data-path
+the C ABI with host buffers (`e2e`), per-stage device times and their HBM fractions, PCG
+ms/solve beside the plain FP64 GPU path, p50/p99 step latency, the solve kernel's roofline,
+clocks, the batched 64-scene workload beside the plain FP64 path (`batch`), and the reference
+CPU step's throughput on a bounded sample (`cpu_baseline`).  `--impl reference` times the
+reference's own FlipSim::Step, compiled from its sources into oracle/_ref with TBB's parallel_for
+spread over the host's threads, on the same workload in the reference's own configuration (the
+oracle's restatement when that build is absent).  Multi-GPU runs are independent replicas (one scene per GPU, no data-path
 collective); only timing scalars cross ranks.
 """
 import argparse
@@ -39,6 +41,17 @@ sys.path.insert(0, ROOT)
 #   REF32 (the reference's two-reduction PCG): 61 per iteration, 35 per solve.
 PCG_BYTES_PER_CELL_ITER = {"fp64": 96.0, "mixed": 48.0, "ref32": 61.0}
 PCG_BYTES_PER_CELL_OUTER = {"fp64": 108.0, "mixed": 80.0, "ref32": 35.0}
+# The fixed per-unit figures the roofline is reported on (bytes per FLUID cell per CG iteration of
+# a two-reduction PCG: SpMV 21 + two axpys 48 + diagonal preconditioner 20 + s-update 24 = 113 in
+# fp64, 61 with fp32 vectors); refinement sweeps as above.
+PCG_SPEC_BYTES_PER_CELL_ITER = {"fp64": 113.0, "mixed": 61.0, "ref32": 61.0}
+# Per-stage algorithmic bytes per particle and per cell (fp32 state): sort 64/p + 8/c (offsets);
+# density 16/p; forces 32/p; P2G 24/p + 24/c (current and previous faces); classify 5/c;
+# boundary + divergence 16/c; gradient 33/c; extrapolate 25/c + the FLIP delta 36/c; G2P + blend +
+# advect 48/p; resampling 48/p plus its own sort.
+STAGE_BYTES = {"sort": (64.0, 8.0), "density": (16.0, 0.0), "forces": (32.0, 0.0), "p2g": (24.0, 24.0),
+               "classify": (0.0, 5.0), "boundary_div": (0.0, 16.0), "gradient": (0.0, 33.0),
+               "extrapolate": (0.0, 61.0), "g2p_advect": (48.0, 0.0), "resample": (112.0, 8.0)}
 STAGE_NAMES = ["begin", "sort", "density", "forces", "p2g", "classify", "boundary_div", "solve",
                "gradient", "extrapolate", "g2p_advect", "resample"]
 
@@ -264,17 +277,49 @@ def fp64_oracle_error(A, Batch, b, desc, tols=(1e-5, 1e-7)):
     return out
 
 
+def reference_sim(A, desc, rng_seed=0x5EED):
+    """The reference's own FlipSim (oracle/_ref, compiled from its sources; TBB's parallel_for on
+    all host threads) when that build is present, else None.  Seeded with the oracle's restatement
+    of Scene::GenerateParticles (scene.cpp needs meshes and OpenVDB)."""
+    try:
+        from oracle import pyref
+        if not pyref.available("omp"):
+            return None
+        from oracle.pyoracle import RefSim
+        seed = RefSim(desc, pyref.reference_params())
+        seed.init()
+        st = seed.get_particles()
+        seed.close()
+        r = pyref.ReferenceSim(desc, rng_seed, variant="omp")
+        r.init_with(st)
+        return r, len(st["mass"]), pyref.threads("omp")
+    except Exception:
+        return None
+
+
+REFERENCE_CONFIG = ("the reference's own configuration: fp32 PCG with its preconditioner to its absolute stop "
+                    "rule r.r <= 1e-2 n^3 (solver.inl:289-354), resampling every step")
+
+
 def reference_arm(args, A, ws, rank):
     if rank != 0:
         return 0
     desc = A.scene_dambreak(args.n, seed=1)
-    from oracle.pyoracle import RefSim, lib as olib
-    prm = make_params(A, A.PREC_REF32, args.tol, timing=0, graph=0)
-    r = RefSim(desc, prm, faithful=True)
-    r.init()
-    n = r.count()
+    ref = reference_sim(A, desc)
     budget = args.ref_budget_s
     done, t_total = 0, 0.0
+    if ref is not None:
+        r, n, cores = ref
+        kind = "reference"
+        what = "the reference's own FlipSim::Step compiled from its sources (oracle/_ref), " + REFERENCE_CONFIG
+    else:
+        from oracle.pyoracle import RefSim, lib as olib
+        r = RefSim(desc, make_params(A, A.PREC_REF32, args.tol, timing=0, graph=0), faithful=True)
+        r.init()
+        n = r.count()
+        cores = olib().ariel_ref_max_threads()
+        kind = "port"
+        what = "the oracle's restatement of the reference step, reference-faithful OpenMP granularity"
     # the CPU needs no warm-up; each timed step is a full FLIP step of the workload, run until
     # K steps or the time budget, whichever comes first
     while done < args.steps:
@@ -284,21 +329,51 @@ def reference_arm(args, A, ws, rank):
         done += 1
         if t_total >= budget:
             break
-    cores = olib().ariel_ref_max_threads()
+    r.close()
     value = n * done / t_total
-    sample = ("%d of %d FLIP steps of the %d^3 dam break (%d particles) from Init, reference-faithful "
-              "OpenMP granularity, %.1f s" % (done, args.steps, args.n, n, t_total))
+    sample = ("frames 1-%d (of %d asked) of the %d^3 dam break (%d particles) from Init: %s; %d threads, %.1f s"
+              % (done, args.steps, args.n, n, what, cores, t_total))
+    cfg = config_dict(args, n, ws)
+    cfg["precision"] = "fp32 (the reference's)" if kind == "reference" else "ref32"
+    cfg["stop_rule"] = "absolute r.r <= 1e-2 n^3 (solver.inl:322)" if kind == "reference" else "relative %g" % args.tol
+    cfg["workload"] = "dam break %d^3, %d particles, %s" % (args.n, n, REFERENCE_CONFIG if kind == "reference"
+                                                              else "fp32 PCG to %g relative residual" % args.tol)
+    cfg["frames"] = [1, done]
+    if kind == "reference":
+        cfg["tolerance"] = None
     line = {
         "impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
         "n_gpus": ws, "steps": done, "warmup": 0, "ms_per_step": 1000.0 * t_total / done,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(args, n, ws),
-        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batch_subresult(A, Batch, args):
+    """BASELINE config 4 beside the headline: the uneven 64-scene batch, MIXED against the plain
+    FP64 path, a few graph-replayed steps each (step and solve ratios)."""
+    from ariel_b200 import workloads as W
+    descs = W.uneven_batch(args.batch_sub, seed=args.seed)
+    res = {}
+    for name, prec in (("mixed", A.PREC_MIXED), ("fp64", A.PREC_FP64)):
+        b, r = run_gpu_pass(A, Batch, descs, make_params(A, prec, args.tol), args.batch_steps, 3)
+        t = r["totals"]
+        res[name] = {"ms_per_step": r["ms"] / args.batch_steps,
+                     "solve_ms": r["timing"]["solve_kernel_ms"] / max(t.solves, 1),
+                     "particle_steps_per_s": r["np"] * args.batch_steps / (r["ms"] / 1000.0)}
+        n = r["np"]
+        b.close()
+    return {"workload": "%d dam-break scenes, grids drawn from {32,48,64,96,128}^3 (seed %d), blocks filling "
+                        "20-50%%, %d particles, PCG to %g relative, frames 4-%d"
+                        % (args.batch_sub, args.seed, n, args.tol, 3 + args.batch_steps),
+            "mixed": res["mixed"], "fp64": res["fp64"],
+            "step_speedup_vs_fp64": res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"],
+            "solve_speedup_vs_fp64": res["fp64"]["solve_ms"] / res["mixed"]["solve_ms"]}
 
 
 def config_dict(args, n_particles, ws):
@@ -317,8 +392,9 @@ def config_dict(args, n_particles, ws):
                 "grid": args.n, "particles_per_scene": n_particles, "precision": args.precision,
                 "tolerance": args.tol, "parallelism": "replicas" if ws > 1 else "single",
                 "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
-    return {"workload": "dam break %d^3, %d particles per scene, mixed-precision PCG to %g relative residual"
-            % (args.n, n_particles, args.tol),
+    pname = {"mixed": "mixed-precision", "fp64": "fp64", "ref32": "fp32"}[args.precision]
+    return {"workload": "dam break %d^3, %d particles per scene, %s PCG to %g relative residual"
+            % (args.n, n_particles, pname, args.tol),
             "grid": args.n, "particles_per_scene": n_particles, "scenes": ws, "precision": args.precision,
             "preconditioner": ("MIC(0), tau 0.97" if args.precond == "mic0" else "reference (solver.inl:104-135)"),
             "tolerance": args.tol, "dt": 1.0 / 240.0,
@@ -413,6 +489,9 @@ def main():
                     help="dambreak: the headline 128^3 scene; sphere: 256^3 with a solid sphere; batch: 64 "
                          "uneven scenes stepped together; serve: Poisson arrivals through the request server")
     ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--batch-sub", type=int, default=64,
+                    help="dambreak: also time this many uneven scenes batched (config 4), MIXED and FP64; 0: off")
+    ap.add_argument("--batch-steps", type=int, default=6)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
     ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
@@ -491,7 +570,9 @@ def main():
     p99 = step_list[min(len(step_list) - 1, int(round(0.99 * (len(step_list) - 1))))] if step_list else None
     solve_ms = tim["solve_kernel_ms"] / max(tot.solves, 1)
     key = args.precision
-    alg_bytes = (tot.cell_iterations * PCG_BYTES_PER_CELL_ITER[key] +
+    alg_bytes = (tot.cell_iterations * PCG_SPEC_BYTES_PER_CELL_ITER[key] +
+                 tot.cell_outer * PCG_BYTES_PER_CELL_OUTER[key]) / max(tot.solves, 1)
+    own_bytes = (tot.cell_iterations * PCG_BYTES_PER_CELL_ITER[key] +
                  tot.cell_outer * PCG_BYTES_PER_CELL_OUTER[key]) / max(tot.solves, 1)
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else None
@@ -505,10 +586,20 @@ def main():
     # FLUID cells of all scenes from the per-scene sweep totals (cell_outer = sum nf * sweeps)
     fluid_cells = tot.cell_outer * b.k / max(tot.outer, 1)
     in_l2 = fluid_cells * (2 * 4 + 2) * (8 if args.precision == "fp64" else 4) < 100e6
-    roofline = {"kernel": "k_pcg<%s> (persistent pressure solve)" % args.precision, "bound": "hbm",
+    roofline = {"kernel": "k_pcg_fast<%s> (persistent pressure solve)" % args.precision, "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
-                "traffic": traffic, "algorithmic_bytes_per_launch": alg_bytes,
+                "traffic": traffic,
+                "traffic_source": ("committed ncu capture of this workload (profiles/traffic.txt), not measured "
+                                   "by this run" if traffic is not None else None),
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "bytes_model": "%g B per FLUID cell per CG iteration (two-reduction PCG, fp%s vectors) + %g B per "
+                               "cell per refinement sweep" % (PCG_SPEC_BYTES_PER_CELL_ITER[key],
+                                                              "64" if key == "fp64" else "32",
+                                                              PCG_BYTES_PER_CELL_OUTER[key]),
+                "achieved_own_model": own_bytes / (solve_ms / 1000.0) / 1e9 if solve_ms > 0 else None,
+                "own_model": "%g B per cell-iteration: the single-reduction algorithm's own traffic"
+                             % PCG_BYTES_PER_CELL_ITER[key],
                 "avg_launch_ms": solve_ms,
                 "note": "frac of %s HBM copy bandwidth; " % peak_kind +
                         ("the solve's working set stays in L2 at this size, so DRAM traffic is far below "
@@ -516,12 +607,27 @@ def main():
                          "the solve's working set exceeds L2: DRAM traffic includes the streamed "
                          "16-byte cell records (about 16 B per FLUID cell per iteration)")}
 
+    # every stage against HBM with its per-particle and per-cell bytes, from the same CUDA-event
+    # stage times (stages with several kernels are timed as one)
+    n_cells = sum(d.dim ** 3 for d in (desc if isinstance(desc, list) else [desc]))
+    stage_roof = {}
+    for name, (bp, bc) in STAGE_BYTES.items():
+        t = stage_ms.get(name)
+        if not t:
+            continue
+        if name == "resample" and resample_every > 1:
+            t = t * resample_every  # the stage runs on one step in resample_every
+        nbytes = bp * n_local + bc * n_cells
+        gbs = nbytes / (t / 1000.0) / 1e9
+        stage_roof[name] = {"ms": t, "bytes": nbytes, "achieved_gbs": gbs, "frac": gbs / peak}
+    cfg = config_dict(args, n_local, ws)
+    cfg["frames"] = [args.warmup + 1, args.warmup + args.steps]
     out = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_dict(args, n_local, ws),
-        "stage_ms": stage_ms, "step_ms_p50": p50, "step_ms_p99": p99,
+        "data": "synthetic", "config": cfg,
+        "stage_ms": stage_ms, "stage_roofline": stage_roof, "step_ms_p50": p50, "step_ms_p99": p99,
         "pcg": {"ms_per_solve": solve_ms, "iterations_per_solve": tot.iterations / max(tot.solves, 1),
                 "outer_per_solve": tot.outer / max(tot.solves, 1), "not_converged": tot.not_converged,
                 "final_rel_residual": res["stats"].pcg_rel_residual},
@@ -554,11 +660,25 @@ def main():
         out["throughput_vs_fp64"] = r64["ms"] / res["ms"] if res["ms"] > 0 else None
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "dambreak":
-        n, dt, cores, st = cpu_baseline_sample(A, desc, args.tol)
-        out["cpu_baseline"] = {"value": n / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
-                               "sample": "1 FLIP step (from Init) of the same %d^3 dam break, %d particles, "
-                                         "reference-faithful OpenMP granularity, fp32 PCG to %g relative "
-                                         "(%d iterations), %.1f s" % (args.n, n, args.tol, st.pcg_iterations, dt)}
+        ref = reference_sim(A, desc)
+        if ref is not None:
+            r, n, cores = ref
+            t0 = time.perf_counter()
+            r.step(1)
+            dt = time.perf_counter() - t0
+            r.close()
+            out["cpu_baseline"] = {"value": n / dt, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+                                   "sample": "frame 1 (from Init) of the same %d^3 dam break, %d particles: the "
+                                             "reference's own FlipSim::Step compiled from its sources (oracle/_ref), "
+                                             "%s; %.1f s" % (args.n, n, REFERENCE_CONFIG, dt)}
+        else:
+            n, dt, cores, st = cpu_baseline_sample(A, desc, args.tol)
+            out["cpu_baseline"] = {"value": n / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                                   "sample": "1 FLIP step (from Init) of the same %d^3 dam break, %d particles, "
+                                             "reference-faithful OpenMP granularity, fp32 PCG to %g relative "
+                                             "(%d iterations), %.1f s" % (args.n, n, args.tol, st.pcg_iterations, dt)}
+    if rank == 0 and ws == 1 and args.batch_sub > 0 and args.workload == "dambreak":
+        out["batch"] = batch_subresult(A, Batch, args)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if pg:

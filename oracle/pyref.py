@@ -18,6 +18,8 @@ REF_DIR = os.environ.get("ARIEL_REFERENCE_DIR", "/root/reference")
 _SO = {
     "default": os.path.join(_HERE, "_ref", "libariel_reference.so"),
     "glm096": os.path.join(_HERE, "_ref", "libariel_reference_glm096.so"),
+    # TBB's parallel_for spread over OpenMP threads: the benchmark's CPU reference arm (timed only)
+    "omp": os.path.join(_HERE, "_ref", "libariel_reference_omp.so"),
 }
 _libs = {}
 
@@ -72,6 +74,7 @@ def lib(variant="default"):
         L.ariel_pin_max_density.argtypes = [vp]
         L.ariel_pin_max_density.restype = C.c_float
         L.ariel_pin_frame.argtypes = [vp]
+        L.ariel_pin_threads.restype = C.c_int32
         L.ariel_pin_philox4x32_10.argtypes = [vp, vp, vp]
         L.ariel_pin_philox4x32_10.restype = None
         _libs[variant] = L
@@ -176,6 +179,10 @@ class ReferenceSim:
 def _arrays(st):
     return (np.ascontiguousarray(st["pos"], np.float32), np.ascontiguousarray(st["vel"], np.float32),
             np.ascontiguousarray(st["mass"], np.float32), np.ascontiguousarray(st["type"], np.int32))
+
+
+def threads(variant="default"):
+    return lib(variant).ariel_pin_threads()
 
 
 def philox(counter, key, variant="default"):

@@ -64,11 +64,13 @@ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 const uint32_t kTagResample = 0x5245534Du;  // "RESM": the resampling jitter's stream
 
 struct RandState {
-    uint64_t seed = 0;
     unsigned int last_n0 = 0xFFFFFFFFu;
     float last_frame = -1.0f;
     uint32_t draws = 0;
-} g_rand;
+};
+uint64_t g_rand_seed = 0;
+// per thread: the timing build's OpenMP workers each draw for their own particles
+thread_local RandState g_rand;
 
 // A null stream buffer: the reference prints every step and every PCG iteration
 // (src/sim/flip.cpp:94, src/sim/solver.inl:336-337); the driver silences std::cout while it runs.
@@ -92,7 +94,7 @@ extern "C" int ariel_pin_rand_draw(unsigned int n0, float frame) {
     }
     uint32_t d = g_rand.draws++;
     uint32_t c[4] = {(uint32_t)n0, (uint32_t)frame, d / 3u, kTagResample};
-    philox4x32_10(c, (uint32_t)g_rand.seed, (uint32_t)(g_rand.seed >> 32));
+    philox4x32_10(c, (uint32_t)g_rand_seed, (uint32_t)(g_rand_seed >> 32));
     return (int)(c[d % 3u] % 101u);
 }
 
@@ -242,7 +244,7 @@ ariel_pin* ariel_pin_create(int32_t n, float density, float dt, const float* for
     h->scene.m_solidLevelSet.m_owner = &h->scene;
     h->scene.m_liquidLevelSet.m_owner = &h->scene;
     g_rand = RandState();
-    g_rand.seed = rng_seed;
+    g_rand_seed = rng_seed;
     Quiet q;
     h->sim = new fluidCore::FlipSim(glm::vec3(n, n, n), density, dt, &h->scene, false);
     return h;
@@ -477,6 +479,15 @@ int32_t ariel_pin_set_grid(ariel_pin* h, int32_t which, const void* buf) {
         for (int j = 0; j < ey; ++j)
             for (int k = 0; k < ez; ++k) g->SetCell(i, j, k, v[t++]);
     return 0;
+}
+
+// Host threads the timing build's parallel_for uses (1 for the serial builds).
+int32_t ariel_pin_threads(void) {
+#if defined(ARIEL_TBB_OPENMP) && defined(_OPENMP)
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
 }
 
 float ariel_pin_max_density(ariel_pin* h) { return h ? h->sim->m_max_density : 0.0f; }

@@ -9,6 +9,9 @@
 
 #include <cstddef>
 #include <vector>
+#if defined(ARIEL_TBB_OPENMP) && defined(_OPENMP)
+#include <omp.h>
+#endif
 
 namespace tbb {
 
@@ -24,10 +27,33 @@ class blocked_range {
     Value m_begin, m_end;
 };
 
+#if defined(ARIEL_TBB_OPENMP) && defined(_OPENMP)
+// Timing build (oracle/_ref/libariel_reference_omp.so, the benchmark's CPU reference arm): the
+// range is cut into one contiguous piece per OpenMP thread, each handed to the body, as TBB's
+// scheduler would cut it across its workers.  The reference's benign races then run as races,
+// as they do under TBB; this build is timed, never compared.
+template <typename Range, typename Body>
+void parallel_for(const Range& range, const Body& body) {
+    typedef decltype(range.begin()) V;
+    const long long b = (long long)range.begin(), e = (long long)range.end();
+    const long long len = e - b;
+    if (len <= 1 || omp_in_parallel()) {
+        body(range);
+        return;
+    }
+#pragma omp parallel
+    {
+        const long long nt = omp_get_num_threads(), t = omp_get_thread_num();
+        const long long lo = b + len * t / nt, hi = b + len * (t + 1) / nt;
+        if (lo < hi) body(Range((V)lo, (V)hi));
+    }
+}
+#else
 template <typename Range, typename Body>
 void parallel_for(const Range& range, const Body& body) {
     body(range);
 }
+#endif
 
 class task {
   public:
