@@ -1,7 +1,7 @@
 """ctypes mirror of include/ariel.h (structs, enums, status codes).
 
 The layouts here must match include/ariel.h field for field; tests/test_abi.py checks the
-sizes against the compiled library's own sizeof().
+sizes and field offsets against the C compiler.s view of the header.
 """
 import ctypes as C
 
@@ -41,6 +41,7 @@ STAGE_NAMES = ["begin", "sort", "density", "forces", "p2g", "classify", "boundar
 MAX_BOXES = 8
 MAX_SPHERES = 8
 MAX_FORCES = 4
+MAX_MESHES = 8
 
 
 class AsimBox(C.Structure):
@@ -58,6 +59,7 @@ class AsimSceneDesc(C.Structure):
         ("n_liquid", C.c_int32), ("liquid", AsimBox * MAX_BOXES),
         ("n_solid", C.c_int32), ("solid", AsimSphere * MAX_SPHERES),
         ("seed", C.c_uint64), ("jitter", C.c_float), ("reserved", C.c_int32),
+        ("n_mesh", C.c_int32), ("mesh", C.c_int32 * MAX_MESHES),
     ]
 
 
@@ -173,6 +175,15 @@ def scene_dambreak(n, liquid_hi=(0.4, 0.6, 1.0), dt=1.0 / 240.0, density=0.5, se
     d.seed = seed
     d.jitter = jitter
     return d
+
+
+def add_mesh(desc, mesh_id):
+    """References a solid mesh (an ariel_mesh_create id) from a scene description."""
+    if desc.n_mesh >= MAX_MESHES:
+        raise ValueError("at most %d meshes per scene" % MAX_MESHES)
+    desc.mesh[desc.n_mesh] = mesh_id
+    desc.n_mesh += 1
+    return desc
 
 
 def status_name(code):

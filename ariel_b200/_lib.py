@@ -18,6 +18,8 @@ SIGNATURES = {
     "ariel_abi_version": ([], C.c_int32),
     "ariel_params_default": ([C.POINTER(A.AsimParams)], None),
     "ariel_scene_dambreak": ([C.POINTER(A.AsimSceneDesc), C.c_int32], None),
+    "ariel_mesh_create": ([_vp, C.c_int32, _vp, C.c_int32, _vp, C.c_float, C.POINTER(C.c_int32)], C.c_int),
+    "ariel_mesh_destroy": ([C.c_int32], C.c_int),
     "ariel_status_string": ([C.c_int], C.c_char_p),
     "ariel_create": ([C.POINTER(A.AsimSceneDesc), C.POINTER(A.AsimParams), C.POINTER(_vp)], C.c_int),
     "ariel_create_batch": ([C.POINTER(A.AsimSceneDesc), C.c_int32, C.POINTER(A.AsimParams), C.POINTER(_vp)], C.c_int),

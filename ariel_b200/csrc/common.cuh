@@ -52,6 +52,10 @@ struct SceneDev {
     float dens_inv_hh;
     int re_pow2;         // resample_re^2 is a power of two
     float re_inv_hh;
+    // static solid meshes: the scene's tree and triangles (mesh.cuh), world coordinates
+    int n_meshes;
+    const struct MeshNode* mesh_nodes;
+    const struct MeshTri* mesh_tris;
 };
 
 // ------------------------------------------------------------------------------------------

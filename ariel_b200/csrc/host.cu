@@ -156,7 +156,7 @@ void free_all(ariel_sim* s) { free_bufs(s, false); }
 
 // Buffer sizes of one packed layout.
 struct Layout {
-    long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0, nbricks = 0;
+    long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0, nbricks = 0, mesh_nodes = 0, mesh_tris = 0;
     bool any_solid = false;
     int mode = kRef32;
 };
@@ -246,6 +246,8 @@ long long layout_bytes(const Layout& L) {
     add(1, sizeof(PcgCtl));
     add(1, sizeof(Barrier));
     add(L.ns, 16);  // solid_pos
+    add(L.mesh_nodes, sizeof(MeshNode));
+    add(L.mesh_tris, sizeof(MeshTri));
     return total;
 }
 
@@ -281,6 +283,10 @@ void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
     const float density = d.density;
     const float w = density * thickness;
     const uint32_t k0 = (uint32_t)d.seed, k1 = (uint32_t)(d.seed >> 32);
+    std::shared_ptr<SceneMeshes> M;
+    if (scene_meshes(d, M) != ARIEL_OK) M = std::make_shared<SceneMeshes>();
+    const MeshNode* mn = M->nodes.empty() ? nullptr : M->nodes.data();
+    const MeshTri* mt = M->tris.empty() ? nullptr : M->tris.data();
     auto inside_solid = [&](float x, float y, float z) {
         for (int s = 0; s < d.n_solid; ++s) {
             float cx = d.solid[s].center[0] * maxdim, cy = d.solid[s].center[1] * maxdim,
@@ -289,7 +295,7 @@ void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
             float dd = (dx * dx + dy * dy) + dz * dz;
             if (dd < r * r) return true;
         }
-        return false;
+        return mesh_inside_bits(mn, mt, make_float3(x, y, z)) != 0u;
     };
     out = HostParticles{};
     for (int l = 0; l < d.n_liquid; ++l) {
@@ -343,6 +349,26 @@ void generate_particles(const AsimSceneDesc& d, HostParticles& out) {
                     out.vel4.push_back(pack_vel(0.0f, 0.0f, 0.0f, ARIEL_SOLID));
                 }
     }
+    // solid meshes after the spheres, each over the lattice of its world bounding box
+    // (scene.cpp:307-332), keeping the points the mesh itself contains
+    for (size_t m = 0; m < M->lo.size(); ++m) {
+        const float3 lo = M->lo[m], hi = M->hi[m];
+        float lminx = hmax(std::floor(lo.x), 0.0f) / density;
+        float lminy = hmax(std::floor(lo.y), 0.0f) / density;
+        float lminz = hmax(std::floor(lo.z), 0.0f) / density;
+        float lmaxx = hmin(std::ceil(hi.x), maxdim + 1.0f) / density;
+        float lmaxy = hmin(std::ceil(hi.y), maxdim + 1.0f) / density;
+        float lmaxz = hmin(std::ceil(hi.z), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    float px = (i * w) + (w / 2.0f), py = (j * w) + (w / 2.0f), pz = (k * w) + (w / 2.0f);
+                    const uint32_t bits = mesh_inside_bits(mn, mt, make_float3(px * maxdim, py * maxdim, pz * maxdim));
+                    if (!((bits >> m) & 1u)) continue;
+                    out.pos4.push_back(make_float4(px, py, pz, 10.0f));
+                    out.vel4.push_back(pack_vel(0.0f, 0.0f, 0.0f, ARIEL_SOLID));
+                }
+    }
     bin_solids(d, out);
 }
 
@@ -378,6 +404,7 @@ SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
     D.n = d.dim;
     D.n_forces = d.n_forces;
     D.n_spheres = d.n_solid;
+    D.n_meshes = d.n_mesh;
     D.frame = 0;
     D.maxd = (float)d.dim;
     D.density = d.density;
@@ -417,6 +444,7 @@ ariel_status validate(const AsimSceneDesc& d) {
     if (d.n_forces < 0 || d.n_forces > ARIEL_MAX_FORCES) return ARIEL_ERR_INVALID_ARG;
     if (d.n_liquid < 0 || d.n_liquid > ARIEL_MAX_BOXES) return ARIEL_ERR_INVALID_ARG;
     if (d.n_solid < 0 || d.n_solid > ARIEL_MAX_SPHERES) return ARIEL_ERR_INVALID_ARG;
+    if (!meshes_valid(d)) return ARIEL_ERR_INVALID_ARG;
     if ((long long)d.dim * d.dim * d.dim > (1ll << 30)) return ARIEL_ERR_INVALID_ARG;
     return ARIEL_OK;
 }
@@ -436,7 +464,11 @@ long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector
         L.nf += 3 * n * n * (n + 1);
         L.ns += solids[i];
         L.maxch += chunk_bound(n * n * n);
-        if (descs[i].n_solid > 0) L.any_solid = true;
+        if (descs[i].n_solid > 0 || descs[i].n_mesh > 0) L.any_solid = true;
+        long long mn = 0, mt = 0;
+        mesh_counts(descs[i], mn, mt);
+        L.mesh_nodes += mn;
+        L.mesh_tris += mt;
     }
     return layout_bytes(L);
 }
@@ -479,7 +511,7 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
         s->sh[i].p_end = s->ppref[i + 1];
         s->sh[i].c_begin = s->cpref[i];
         s->sh[i].f_begin = s->fpref[i];
-        if (s->descs[i].n_solid > 0) s->any_solid = true;
+        if (s->descs[i].n_solid > 0 || s->descs[i].n_mesh > 0) s->any_solid = true;
         maxch += chunk_bound(n * n * n);
     }
     s->np = s->ppref[k];
@@ -617,6 +649,30 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     ARIEL_TRY(dalloc(s, &A.ctl, 1));
     ARIEL_TRY(dalloc(s, &A.bar, 1));
     ARIEL_TRY(dalloc(s, &S.solid_pos, s->spref[k], true));
+    // solid meshes: every scene's tree and triangles back to back
+    {
+        long long tn = 0, tt = 0;
+        for (int i = 0; i < k; ++i) {
+            tn += (long long)s->meshes[i]->nodes.size();
+            tt += (long long)s->meshes[i]->tris.size();
+        }
+        ARIEL_TRY(dalloc(s, &s->d_mesh_nodes, tn));
+        ARIEL_TRY(dalloc(s, &s->d_mesh_tris, tt));
+        long long on = 0, ot = 0;
+        for (int i = 0; i < k; ++i) {
+            const SceneMeshes& M = *s->meshes[i];
+            s->sh[i].mesh_nodes = M.nodes.empty() ? nullptr : s->d_mesh_nodes + on;
+            s->sh[i].mesh_tris = M.tris.empty() ? nullptr : s->d_mesh_tris + ot;
+            if (!M.nodes.empty()) {
+                ARIEL_CUDA(copy_sync(s->stream, s->d_mesh_nodes + on, M.nodes.data(), M.nodes.size() * sizeof(MeshNode),
+                                     cudaMemcpyHostToDevice));
+                ARIEL_CUDA(copy_sync(s->stream, s->d_mesh_tris + ot, M.tris.data(), M.tris.size() * sizeof(MeshTri),
+                                     cudaMemcpyHostToDevice));
+            }
+            on += (long long)M.nodes.size();
+            ot += (long long)M.tris.size();
+        }
+    }
     A.S = S;
     s->pcg_blocks = pcg_max_blocks(s->device, s->mode, s->prm.pcg_blocks_per_sm);
     if (s->prm.pcg_grid_blocks > 0) s->pcg_blocks = std::min(s->pcg_blocks, (int)s->prm.pcg_grid_blocks);
@@ -761,6 +817,14 @@ ariel_status new_sim(const AsimSceneDesc* descs, int k, const AsimParams& prm, c
     s->prm = prm;
     s->frames.assign(k, 0);
     for (int i = 0; i < k; ++i) s->sh.push_back(make_scene(descs[i], prm));
+    s->meshes.resize(k);
+    for (int i = 0; i < k; ++i) {
+        ariel_status ms = scene_meshes(descs[i], s->meshes[i]);
+        if (ms != ARIEL_OK) {
+            delete s;
+            return ms;
+        }
+    }
     s->pool = pool;
     if (stream) {
         s->stream = stream;

@@ -7,6 +7,7 @@
 // ascending, particles inside a cell in ascending particle id (the order ParticleGrid::Sort
 // appends them, particlegrid.cpp:150-171).  The cell sort therefore finishes each cell's
 // segment with an insertion sort by id after the arrival-order scatter.
+#include "mesh.cuh"
 #include "state.cuh"
 
 namespace ariel {
@@ -18,14 +19,16 @@ namespace {
     load_prefix<kMaxScenes>(pref_s, (pref_src), S.k)
 
 // ------------------------------------------------------------------------------------------
-// Analytic spheres (replaces Scene::IntersectSolidGeoms scene.cpp:425-434,
-// CheckPointInsideSolidGeom scene.cpp:382-402, LevelSet::ProjectPointsToSurface
-// levelset.cpp:175-193).  World (grid) units.
+// Solids: analytic spheres, then static meshes (mesh.cuh), replacing
+// Scene::IntersectSolidGeoms scene.cpp:425-434, CheckPointInsideSolidGeom scene.cpp:382-402 and
+// LevelSet::ProjectPointsToSurface levelset.cpp:175-193.  World (grid) units.
 // ------------------------------------------------------------------------------------------
 struct Hit {
     bool hit;
     float3 point, normal;
 };
+
+__device__ __forceinline__ bool has_solids(const SceneDev& D) { return D.n_spheres > 0 || D.n_meshes > 0; }
 
 __device__ bool inside_solid(const SceneDev& D, float3 p) {
     for (int i = 0; i < D.n_spheres; ++i) {
@@ -33,7 +36,7 @@ __device__ bool inside_solid(const SceneDev& D, float3 p) {
         float3 d = f3sub(p, make_float3(s.x, s.y, s.z));
         if (gdot3(d, d) < s.w * s.w) return true;
     }
-    return false;
+    return D.n_meshes > 0 && mesh_inside_bits(D.mesh_nodes, D.mesh_tris, p) != 0u;
 }
 
 __device__ Hit intersect_solids(const SceneDev& D, float3 o, float3 dir) {
@@ -61,6 +64,20 @@ __device__ Hit intersect_solids(const SceneDev& D, float3 o, float3 dir) {
             bestd = d;
         }
     }
+    if (D.n_meshes > 0) {
+        // solid meshes after the spheres, as the scene lists its solids (scene.cpp:425-434)
+        float3 pt;
+        float d;
+        const int t = mesh_nearest(D.mesh_nodes, D.mesh_tris, o, dir, pt, d);
+        if (t >= 0 && (!best.hit || !(bestd <= d))) {
+            const MeshTri& T = D.mesh_tris[t];
+            const float3 v0 = m3(T.v0);
+            best.hit = true;
+            best.point = pt;
+            best.normal = mnormalize(mcross(msub(m3(T.v1), v0), msub(m3(T.v2), v0)));
+            bestd = d;
+        }
+    }
     return best;
 }
 
@@ -71,6 +88,8 @@ __device__ float3 closest_solid_surface(const SceneDev& D, float3 p) {
         float3 d = f3sub(p, c);
         if (gdot3(d, d) < s.w * s.w) return f3add(c, f3mul(gnormalize3(d), s.w));
     }
+    float3 q;
+    if (D.n_meshes > 0 && mesh_closest(D.mesh_nodes, D.mesh_tris, p, q) >= 0) return q;
     return p;
 }
 
@@ -115,7 +134,7 @@ __global__ void k_begin_solids(DevState S) {
     const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
     float4 p4 = S.pos4[g];
     float4 v4 = S.vel4[g];
-    if (D.n_spheres > 0 && type_of(v4) == ARIEL_FLUID) {
+    if (has_solids(D) && type_of(v4) == ARIEL_FLUID) {
         const float maxd = D.maxd;
         float3 p = make_float3(p4.x, p4.y, p4.z);
         if (inside_solid(D, f3mul(p, maxd))) {
@@ -451,7 +470,7 @@ __global__ void k_g2p_advect(DevState S) {
         p.x = gmax(r, gmin(1.0f - r, p.x));
         p.y = gmax(r, gmin(1.0f - r, p.y));
         p.z = gmax(r, gmin(1.0f - r, p.z));
-        if (D.n_spheres > 0) {
+        if (has_solids(D)) {
             // solid push-out against the static SOLID particles of the 27 cells
             const float maxd = D.maxd;
             unsigned ci = (unsigned)gmin((float)n - 1.0f, p.x * maxd);
@@ -718,11 +737,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
     const float4 p4 = S.spos4[s];
     float3 p = make_float3(p4.x, p4.y, p4.z);
     float3 u = make_float3(v4.x, v4.y, v4.z);
-    if (!(D.n_spheres > 0 && inside_solid(D, f3mul(t, maxd)))) {
+    if (!(has_solids(D) && inside_solid(D, f3mul(t, maxd)))) {
         p = t;
         u = ru;
     }
-    if (D.n_spheres > 0)
+    if (has_solids(D))
         solid_constraints(D, p, u, make_float3(p4.x, p4.y, p4.z), make_float3(v4.x, v4.y, v4.z));
     const uint32_t g = S.sid[s];
     S.pos4[g] = make_float4(p.x, p.y, p.z, p4.w);

@@ -5,10 +5,12 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
 
+#include "mesh.cuh"
 #include "pcg.cuh"
 
 namespace ariel {
@@ -24,6 +26,14 @@ struct DeviceBuf {
     size_t bytes = 0;
     bool keep = false;    // persistent state: survives a re-layout until the handle is deleted
     bool pooled = false;  // from the handle's stream-ordered memory pool
+};
+
+// One scene's static solid meshes in world (grid) coordinates behind one tree (mesh.cu), and
+// each mesh's world bounding box (the seeding lattice's range).
+struct SceneMeshes {
+    std::vector<MeshNode> nodes;
+    std::vector<MeshTri> tris;
+    std::vector<float3> lo, hi;
 };
 
 // Host copy of one scene's particles (id order) used while (re)building packed state.
@@ -74,6 +84,9 @@ struct ariel_sim {
     std::vector<AsimSceneDesc> descs;
     AsimParams prm{};
     std::vector<ariel::SceneDev> sh;  // host mirror of the scene table
+    std::vector<std::shared_ptr<ariel::SceneMeshes>> meshes;  // per scene (empty without meshes)
+    ariel::MeshNode* d_mesh_nodes = nullptr;
+    ariel::MeshTri* d_mesh_tris = nullptr;
     std::vector<long long> ppref, cpref, fpref, spref;
     long long np = 0, nc = 0, nf = 0;
     bool any_solid = false;
@@ -123,6 +136,11 @@ ariel_status validate(const AsimSceneDesc& d);
 SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p);
 // Scene::GenerateParticles for one scene, then bin_solids.
 void generate_particles(const AsimSceneDesc& d, HostParticles& out);
+// Solid meshes (mesh.cu): every id of d registered; node and triangle counts of d's tree; the
+// tree itself.
+bool meshes_valid(const AsimSceneDesc& d);
+void mesh_counts(const AsimSceneDesc& d, long long& nodes, long long& tris);
+ariel_status scene_meshes(const AsimSceneDesc& d, std::shared_ptr<SceneMeshes>& out);
 void bin_solids(const AsimSceneDesc& d, HostParticles& hp);
 
 // A handle with its stream and events but no device state.  `stream`/`pool` may be null (own

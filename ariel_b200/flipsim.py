@@ -313,3 +313,31 @@ class Server:
             self.shutdown()
         except Exception:
             pass
+
+
+class Mesh:
+    """A static solid mesh registered with the library (ariel_mesh_create): triangles in object
+    space placed in the unit cube as object * scale + translate; reference it from a scene with
+    `_abi.add_mesh(desc, mesh.id)`."""
+
+    def __init__(self, vertices, triangles, translate=(0.0, 0.0, 0.0), scale=1.0):
+        self.L = lib()
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+        tr = np.ascontiguousarray(translate, np.float32).reshape(3)
+        mid = C.c_int32()
+        check(self.L.ariel_mesh_create(_p(v), len(v), _p(t), len(t), _p(tr), float(scale), C.byref(mid)),
+              "ariel_mesh_create")
+        self.id = mid.value
+        self.vertices, self.triangles, self.translate, self.scale = v, t, tr, float(scale)
+
+    def close(self):
+        if getattr(self, "id", None) is not None:
+            self.L.ariel_mesh_destroy(self.id)
+            self.id = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

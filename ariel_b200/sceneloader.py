@@ -12,12 +12,14 @@ Supported, as the reference reads them:
   of frame 0 (its first mesh under its first transform);
 - ``sim``: {geom, type: "liquid" | "solid", velocity}.
 
-A liquid becomes an AsimBox and a solid an AsimSphere (or a box solid is refused): the GPU path
-seeds and tests analytic boxes and spheres, which is what the reference's box and sphere
-generators tessellate.  Anything the path cannot represent -- OBJ mesh files, animated meshes,
-rotations, non-uniform scaling of spheres, liquids that appear after frame 0, non-cubic grids,
-more boxes, spheres or forces than the ABI holds -- raises ``SceneError`` rather than being
-approximated.  Camera settings are ignored (no viewer).
+A liquid becomes an AsimBox.  A sphere solid becomes an analytic AsimSphere; a box solid and a
+solid read from an OBJ file (``meshfiles`` {id, file}, src/geom/obj/obj.cpp) become static solid
+meshes registered with the library (``ariel_mesh_create``, uniform scale and translation), so
+the returned ``info["meshes"]`` must stay alive while handles are created from the scene.
+Anything the path cannot represent -- liquids from meshes, animated meshes, rotations,
+non-uniform scaling of spheres or meshes, geometry that appears after frame 0, non-cubic grids,
+more boxes, spheres, meshes or forces than the ABI holds -- raises ``SceneError`` rather than
+being approximated.  Camera settings are ignored (no viewer).
 """
 import json
 import os
@@ -27,6 +29,42 @@ from . import _abi as A
 
 class SceneError(ValueError):
     pass
+
+
+def read_obj(path):
+    """Vertices and triangles of an OBJ file (``v`` and ``f`` records; 1-based or negative
+    indices, ``a/b/c`` forms; polygons split into fans, so a quad v0 v1 v2 v3 gives the two
+    triangles the reference tests, Obj::QuadTest obj.cpp:344-352)."""
+    verts, tris = [], []
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            if not parts:
+                continue
+            if parts[0] == "v" and len(parts) >= 4:
+                verts.append([float(parts[1]), float(parts[2]), float(parts[3])])
+            elif parts[0] == "f" and len(parts) >= 4:
+                idx = []
+                for tok in parts[1:]:
+                    i = int(tok.split("/")[0])
+                    idx.append(i - 1 if i > 0 else len(verts) + i)
+                for j in range(1, len(idx) - 1):
+                    tris.append([idx[0], idx[j], idx[j + 1]])
+    if not verts or not tris:
+        raise SceneError("OBJ file %r has no triangles" % path)
+    return verts, tris
+
+
+def _box_mesh(lo, hi):
+    v = [[(lo, hi)[x][0], (lo, hi)[y][1], (lo, hi)[z][2]] for x in (0, 1) for y in (0, 1) for z in (0, 1)]
+    i = lambda x, y, z: x * 4 + y * 2 + z
+    quads = [(i(0, 0, 0), i(0, 1, 0), i(0, 1, 1), i(0, 0, 1)), (i(1, 0, 0), i(1, 0, 1), i(1, 1, 1), i(1, 1, 0)),
+             (i(0, 0, 0), i(0, 0, 1), i(1, 0, 1), i(1, 0, 0)), (i(0, 1, 0), i(1, 1, 0), i(1, 1, 1), i(0, 1, 1)),
+             (i(0, 0, 0), i(1, 0, 0), i(1, 1, 0), i(0, 1, 0)), (i(0, 0, 1), i(0, 1, 1), i(1, 1, 1), i(1, 0, 1))]
+    tris = []
+    for a, b, c, d in quads:
+        tris += [[a, b, c], [a, c, d]]
+    return v, tris
 
 
 def _vec(obj, key, default):
@@ -67,7 +105,8 @@ def scene_from_json(root, jitter=0.0, seed=1, base_dir=""):
         if "id" not in m or m["id"] in meshes:
             continue
         if "file" in m:
-            raise SceneError("mesh file %r: only box and sphere generators are supported" % m["file"])
+            meshes[m["id"]] = ("obj",) + tuple(read_obj(os.path.join(base_dir, m["file"])))
+            continue
         gen = m.get("mesh_gen")
         if gen == "box":
             meshes[m["id"]] = ("box", _vec(m, "point0", (0, 0, 0)), _vec(m, "point1", (0, 0, 0)))
@@ -97,6 +136,10 @@ def scene_from_json(root, jitter=0.0, seed=1, base_dir=""):
             raise SceneError("non-positive scale")
         mesh = geom["mesh"]
         t = (tx, ty, tz)
+        if mesh[0] == "obj":
+            if not (scale[0] == scale[1] == scale[2]):
+                raise SceneError("non-uniformly scaled mesh")
+            return ("obj", mesh[1], mesh[2], t, scale[0])
         if mesh[0] == "box":
             lo = [t[a] + scale[a] * min(mesh[1][a], mesh[2][a]) for a in range(3)]
             hi = [t[a] + scale[a] * max(mesh[1][a], mesh[2][a]) for a in range(3)]
@@ -117,6 +160,7 @@ def scene_from_json(root, jitter=0.0, seed=1, base_dir=""):
         for a, key in enumerate("xyz"):
             d.forces[i][a] = float(fo.get(key, 0.0))
     nl = ns = 0
+    meshes_alive = []
     for node in root.get("sim", []):
         geom = geoms[node["geom"]]
         if geom["offset"] != 0:
@@ -135,15 +179,27 @@ def scene_from_json(root, jitter=0.0, seed=1, base_dir=""):
                 d.liquid[nl].vel[a] = vel[a]
             nl += 1
         elif node.get("type") == "solid":
-            if kind != "sphere":
-                raise SceneError("only sphere solids are supported")
-            if ns >= A.MAX_SPHERES:
-                raise SceneError("more than %d solids" % A.MAX_SPHERES)
-            c, r = shape
-            for a in range(3):
-                d.solid[ns].center[a] = c[a] / n
-            d.solid[ns].radius = r / n
-            ns += 1
+            if kind == "sphere":
+                if ns >= A.MAX_SPHERES:
+                    raise SceneError("more than %d sphere solids" % A.MAX_SPHERES)
+                c, r = shape
+                for a in range(3):
+                    d.solid[ns].center[a] = c[a] / n
+                d.solid[ns].radius = r / n
+                ns += 1
+            else:
+                # a box or OBJ solid: a static mesh in grid units, placed in the unit cube
+                if d.n_mesh >= A.MAX_MESHES:
+                    raise SceneError("more than %d mesh solids" % A.MAX_MESHES)
+                from .flipsim import Mesh
+                if kind == "box":
+                    verts, tris = _box_mesh(*shape)
+                    mesh = Mesh(verts, tris, translate=(0.0, 0.0, 0.0), scale=1.0 / n)
+                else:
+                    verts, tris, t, sc = shape
+                    mesh = Mesh(verts, tris, translate=[x / n for x in t], scale=sc / n)
+                meshes_alive.append(mesh)
+                A.add_mesh(d, mesh.id)
         else:
             raise SceneError("sim node type %r is not supported" % node.get("type"))
     d.n_liquid = nl
@@ -152,5 +208,6 @@ def scene_from_json(root, jitter=0.0, seed=1, base_dir=""):
     d.jitter = jitter
     info = {"dim": n, "density": density, "step_size": step,
             "partio_output": settings.get("partio_output", ""),
-            "vdb_output": settings.get("vdb_output", ""), "mesh_output": settings.get("mesh_output", "")}
+            "vdb_output": settings.get("vdb_output", ""), "mesh_output": settings.get("mesh_output", ""),
+            "meshes": meshes_alive}
     return d, info

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define ARIEL_ABI_VERSION 1
+#define ARIEL_ABI_VERSION 2
 
 typedef enum ariel_status {
     ARIEL_OK = 0,
@@ -103,6 +103,7 @@ enum {
 #define ARIEL_MAX_BOXES 8
 #define ARIEL_MAX_SPHERES 8
 #define ARIEL_MAX_FORCES 4
+#define ARIEL_MAX_MESHES 8
 
 /* Axis-aligned liquid block in unit coordinates (a `mesh_gen` box of the reference's scenes,
  * src/scene/sceneloader.cpp:346-398), with its starting velocity (scene.cpp:280). */
@@ -133,6 +134,8 @@ typedef struct AsimSceneDesc {
     uint64_t seed;        /* seeds the in-sub-cell jitter of the initial liquid lattice */
     float jitter;         /* 1: uniform jitter inside each lattice sub-cell; 0: sub-cell centres */
     int32_t reserved;
+    int32_t n_mesh;       /* static solid meshes (ariel_mesh_create ids), after the spheres */
+    int32_t mesh[ARIEL_MAX_MESHES];
 } AsimSceneDesc;
 
 typedef struct AsimParams {
@@ -263,6 +266,21 @@ ariel_status ariel_timing_get(ariel_sim* sim, double* ms, double* solve_kernel_m
  * that it must time out after `timeout_ms`; returns ARIEL_ERR_DEVICE_TIMEOUT when the bound
  * worked and ARIEL_OK if the barrier (wrongly) completed. */
 ariel_status ariel_selftest_barrier_timeout(double timeout_ms);
+
+/* Static solid meshes: the reference's solid mesh geoms (Scene's solids built from OBJ files,
+ * src/scene/scene.cpp:362-434, src/geom/obj/obj.cpp) for scenes that reference them through
+ * AsimSceneDesc.mesh.  `vertices` holds n_vertices xyz triples in object space, `triangles`
+ * n_triangles index triples (0-based, quads split by the caller); the mesh is placed in the unit
+ * cube as object * scale + translate (uniform scale and translation; rotations are not
+ * supported).  A solid mesh contains a point when a ray from it along +z crosses the mesh an odd
+ * number of times (Scene::CheckPointInsideSolidGeom, scene.cpp:382-402); it yields SOLID
+ * particles at the lattice points inside it and takes part in the solid constraints.  The
+ * library keeps its own copy; host-side only (no device needed), thread-safe.  Limits: at most
+ * 2^24 triangles per mesh.  A scene keeps working with a mesh destroyed after its handle was
+ * created, but new handles referencing a destroyed id are refused. */
+ariel_status ariel_mesh_create(const float* vertices, int32_t n_vertices, const int32_t* triangles,
+                               int32_t n_triangles, const float* translate, float scale, int32_t* mesh_id);
+ariel_status ariel_mesh_destroy(int32_t mesh_id);
 
 /* Checkpoints: every piece of state a step reads from the previous one (particles, pressure
  * warm start, frame counter, density normaliser) of every scene of the handle, in one file.

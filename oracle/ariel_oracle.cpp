@@ -127,6 +127,13 @@ struct Hit {
     vec3 point, normal;
 };
 
+// A static solid mesh's triangle in world (grid) coordinates, with its mesh and its index across
+// the scene's meshes (the tie-break key).
+struct MTri {
+    vec3 a, b, c;
+    int mesh, key;
+};
+
 }  // namespace
 
 struct ariel_ref {
@@ -150,6 +157,8 @@ struct ariel_ref {
     int frame = 0;
     bool inited = false;
     std::vector<Sphere> solids;
+    std::vector<MTri> mtris;         // solid meshes, brute force (no tree)
+    std::vector<vec3> mlo, mhi;      // per mesh world bounding box
     AsimStats st{};
     double stage_ms[ARIEL_STAGE_COUNT] = {};
 };
@@ -163,12 +172,64 @@ using Sim = ariel_ref;
 // CheckPointInsideSolidGeom scene.cpp:382-402 and the OpenVDB closest-point projection
 // levelset.cpp:175-193).  All in world (grid) units.
 // ---------------------------------------------------------------------------------------------
+// Static solid meshes, by brute force over every triangle (the CUDA library walks a tree; the
+// results must not depend on it).  Ray-triangle test: Obj::RayTriangleTest
+// (src/geom/obj/obj.cpp:354-398) with glm::cross / glm::dot as glm writes them.
+inline vec3 gcross(vec3 x, vec3 y) {
+    return mk(x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y);
+}
+bool TriRay(const MTri& T, vec3 o, vec3 d, float& t) {
+    vec3 e1 = T.b - T.a, e2 = T.c - T.a;
+    vec3 pvec = gcross(d, e2);
+    float det = gdot(e1, pvec);
+    if (det == 0.0f) return false;
+    float inv_det = 1.0f / det;
+    vec3 tvec = o - T.a;
+    float bx = gdot(tvec, pvec) * inv_det;
+    vec3 qvec = gcross(tvec, e1);
+    float by = gdot(d, qvec) * inv_det;
+    t = gdot(e2, qvec) * inv_det;
+    return bx >= 0.0f && by >= 0.0f && (bx + by) <= 1.0f;
+}
+// Closest point of a triangle (Ericson, Real-Time Collision Detection, 2005, section 5.1.5).
+vec3 TriClosest(const MTri& T, vec3 p) {
+    vec3 a = T.a, b = T.b, c = T.c;
+    vec3 ab = b - a, ac = c - a, ap = p - a;
+    float d1 = gdot(ab, ap), d2 = gdot(ac, ap);
+    if (d1 <= 0.0f && d2 <= 0.0f) return a;
+    vec3 bp = p - b;
+    float d3 = gdot(ab, bp), d4 = gdot(ac, bp);
+    if (d3 >= 0.0f && d4 <= d3) return b;
+    float vc = d1 * d4 - d3 * d2;
+    if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) return a + ab * (d1 / (d1 - d3));
+    vec3 cp = p - c;
+    float d5 = gdot(ab, cp), d6 = gdot(ac, cp);
+    if (d6 >= 0.0f && d5 <= d6) return c;
+    float vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) return a + ac * (d2 / (d2 - d6));
+    float va = d3 * d6 - d5 * d4;
+    if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f)
+        return b + (c - b) * ((d4 - d3) / ((d4 - d3) + (d5 - d6)));
+    float denom = 1.0f / ((va + vb) + vc);
+    return (a + ab * (vb * denom)) + ac * (vc * denom);
+}
+// Scene::CheckPointInsideSolidGeom (scene.cpp:382-402): odd hit count along +z, per mesh.
+uint32_t MeshInsideBits(const Sim& s, vec3 p) {
+    uint32_t bits = 0;
+    for (const MTri& T : s.mtris) {
+        float t;
+        if (TriRay(T, p, mk(0, 0, 1), t) && t > 0.0f) bits ^= 1u << (T.mesh & 31);
+    }
+    return bits;
+}
+bool HasSolids(const Sim& s) { return !s.solids.empty() || !s.mtris.empty(); }
+
 bool InsideSolid(const Sim& s, vec3 p) {
     for (const Sphere& sp : s.solids) {
         vec3 d = p - sp.c;
         if (gdot(d, d) < sp.r * sp.r) return true;
     }
-    return false;
+    return !s.mtris.empty() && MeshInsideBits(s, p) != 0u;
 }
 
 Hit IntersectSolids(const Sim& s, vec3 o, vec3 dir) {
@@ -193,6 +254,28 @@ Hit IntersectSolids(const Sim& s, vec3 o, vec3 dir) {
             bestd = d;
         }
     }
+    // solid meshes after the spheres: the nearest triangle hit (t > 0), ties to the lower key
+    int bt = -1;
+    float bdist = 0.0f;
+    vec3 bpt = mk(0, 0, 0);
+    for (size_t i = 0; i < s.mtris.size(); ++i) {
+        const MTri& T = s.mtris[i];
+        float t;
+        if (!TriRay(T, o, dir, t) || !(t > 0.0f)) continue;
+        vec3 pt = o + dir * t;
+        vec3 dv = pt - o;
+        float dd = std::sqrt(gdot(dv, dv));
+        if (bt < 0 || dd < bdist || (dd == bdist && T.key < s.mtris[bt].key)) {
+            bt = (int)i;
+            bdist = dd;
+            bpt = pt;
+        }
+    }
+    if (bt >= 0 && (!best.hit || !(bestd <= bdist))) {
+        const MTri& T = s.mtris[bt];
+        best = Hit{true, bpt, gnormalize(gcross(T.b - T.a, T.c - T.a))};
+        bestd = bdist;
+    }
     return best;
 }
 
@@ -201,7 +284,22 @@ vec3 ClosestSolidSurface(const Sim& s, vec3 p) {
         vec3 d = p - sp.c;
         if (gdot(d, d) < sp.r * sp.r) return sp.c + gnormalize(d) * sp.r;
     }
-    return p;
+    // solid meshes: the closest surface point, ties to the lower key
+    int bt = -1;
+    float bd = 0.0f;
+    vec3 q = p;
+    for (size_t i = 0; i < s.mtris.size(); ++i) {
+        const MTri& T = s.mtris[i];
+        vec3 c = TriClosest(T, p);
+        vec3 e = p - c;
+        float d2 = gdot(e, e);
+        if (bt < 0 || d2 < bd || (d2 == bd && T.key < s.mtris[bt].key)) {
+            bt = (int)i;
+            bd = d2;
+            q = c;
+        }
+    }
+    return q;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1260,7 +1358,7 @@ inline vec3 InterpolateVelocity(vec3 p, const Grid<float>& gx, const Grid<float>
 
 // FlipSim::CheckParticleSolidConstraints (flip.cpp:183-227) with analytic solids.
 void CheckParticleSolidConstraints(Sim& s) {
-    if (s.solids.empty()) return;
+    if (!HasSolids(s)) return;
     const float maxd = s.maxd;
     const long np = (long)s.parts.size();
 #pragma omp parallel for schedule(static)
@@ -1293,7 +1391,7 @@ void CheckParticleSolidConstraints(Sim& s) {
 
 // FlipSim::AdjustParticlesStuckInSolids (flip.cpp:130-181) with analytic solids.
 void AdjustParticlesStuckInSolids(Sim& s) {
-    if (s.solids.empty()) return;
+    if (!HasSolids(s)) return;
     const float maxd = s.maxd;
     const long np = (long)s.parts.size();
     for (long p = 0; p < np; ++p) {
@@ -1351,7 +1449,7 @@ void SolvePicFlipAndAdvect(Sim& s) {
         }
         // The reference queries the 27 neighbour cells of every FLUID particle even when no
         // SOLID particle exists; the faithful (timed) mode keeps that cost.
-        if (P.type == ARIEL_FLUID && (s.faithful || !s.solids.empty())) {
+        if (P.type == ARIEL_FLUID && (s.faithful || HasSolids(s))) {
             unsigned i = (unsigned)gmin(x - 1.0f, P.p.x * maxd);
             unsigned j = (unsigned)gmin(y - 1.0f, P.p.y * maxd);
             unsigned k = (unsigned)gmin(z - 1.0f, P.p.z * maxd);
@@ -1534,6 +1632,30 @@ void GenerateParticles(Sim& s) {
                     solid.push_back(p);
                 }
     }
+    // solid meshes after the spheres, each over the lattice of its world bounding box
+    for (size_t m = 0; m < s.mlo.size(); ++m) {
+        vec3 lo = s.mlo[m], hi = s.mhi[m];
+        float lminx = gmax(std::floor(lo.x), 0.0f) / density;
+        float lminy = gmax(std::floor(lo.y), 0.0f) / density;
+        float lminz = gmax(std::floor(lo.z), 0.0f) / density;
+        float lmaxx = gmin(std::ceil(hi.x), maxdim + 1.0f) / density;
+        float lmaxy = gmin(std::ceil(hi.y), maxdim + 1.0f) / density;
+        float lmaxz = gmin(std::ceil(hi.z), maxdim + 1.0f) / density;
+        for (unsigned i = (unsigned)lminx; i < (unsigned)lmaxx; ++i)
+            for (unsigned j = (unsigned)lminy; (float)j < lmaxy; ++j)
+                for (unsigned k = (unsigned)lminz; (float)k < lmaxz; ++k) {
+                    vec3 c = mk((i * w) + (w / 2.0f), (j * w) + (w / 2.0f), (k * w) + (w / 2.0f));
+                    if (!((MeshInsideBits(s, c * maxdim) >> m) & 1u)) continue;
+                    Particle p{};
+                    p.p = c;
+                    p.u = mk(0, 0, 0);
+                    p.n = mk(0, 0, 0);
+                    p.density = 10.0f;
+                    p.type = ARIEL_SOLID;
+                    p.mass = 10.0f;
+                    solid.push_back(p);
+                }
+    }
     s.parts = liquid;
     s.parts.insert(s.parts.end(), solid.begin(), solid.end());
 }
@@ -1676,6 +1798,36 @@ ariel_status ariel_ref_create(const AsimSceneDesc* desc, const AsimParams* param
 }
 
 void ariel_ref_destroy(ariel_ref* r) { delete r; }
+
+ariel_status ariel_ref_add_mesh(ariel_ref* r, const float* vertices, int32_t n_vertices, const int32_t* triangles,
+                                int32_t n_triangles, const float* translate, float scale) {
+    if (!r || !vertices || !triangles || !translate || n_vertices < 3 || n_triangles < 1 || r->inited)
+        return ARIEL_ERR_INVALID_ARG;
+    const float maxd = r->maxd;
+    const int mesh = (int)r->mlo.size();
+    int key = (int)r->mtris.size();
+    auto world = [&](int vi) {
+        return mk((vertices[3 * vi] * scale + translate[0]) * maxd, (vertices[3 * vi + 1] * scale + translate[1]) * maxd,
+                  (vertices[3 * vi + 2] * scale + translate[2]) * maxd);
+    };
+    vec3 lo = mk(3.0e38f, 3.0e38f, 3.0e38f), hi = mk(-3.0e38f, -3.0e38f, -3.0e38f);
+    for (int t = 0; t < n_triangles; ++t) {
+        MTri T;
+        T.a = world(triangles[3 * t]);
+        T.b = world(triangles[3 * t + 1]);
+        T.c = world(triangles[3 * t + 2]);
+        T.mesh = mesh;
+        T.key = key++;
+        for (vec3 v : {T.a, T.b, T.c}) {
+            lo = mk(std::min(lo.x, v.x), std::min(lo.y, v.y), std::min(lo.z, v.z));
+            hi = mk(std::max(hi.x, v.x), std::max(hi.y, v.y), std::max(hi.z, v.z));
+        }
+        r->mtris.push_back(T);
+    }
+    r->mlo.push_back(lo);
+    r->mhi.push_back(hi);
+    return ARIEL_OK;
+}
 void ariel_ref_set_faithful(ariel_ref* r, int32_t f) { r->faithful = f != 0; }
 void ariel_ref_set_threads(int32_t nthreads) {
     if (nthreads > 0) omp_set_num_threads(nthreads);

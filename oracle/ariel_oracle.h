@@ -29,6 +29,10 @@ typedef struct ariel_ref ariel_ref;
 ariel_status ariel_ref_create(const AsimSceneDesc* desc, const AsimParams* params,
                               ariel_ref** out);
 void ariel_ref_destroy(ariel_ref* r);
+/* A static solid mesh (before init): triangles in object space placed at object * scale +
+ * translate in the unit cube, after the scene's spheres; queried by brute force. */
+ariel_status ariel_ref_add_mesh(ariel_ref* r, const float* vertices, int32_t n_vertices, const int32_t* triangles,
+                                int32_t n_triangles, const float* translate, float scale);
 /* 1: the reference's own parallel granularity (one parallel region per (j,k) line in Op,
  *    the S copy and the backward sweep, serial Sort and Product) -- the timed CPU baseline.
  * 0: one parallel region per loop nest (same results, faster; used by the tests). */

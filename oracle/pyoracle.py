@@ -33,6 +33,7 @@ def lib():
         L.ariel_ref_create.argtypes = [C.POINTER(A.AsimSceneDesc), C.POINTER(A.AsimParams), C.POINTER(vp)]
         L.ariel_ref_destroy.argtypes = [vp]
         L.ariel_ref_destroy.restype = None
+        L.ariel_ref_add_mesh.argtypes = [vp, vp, C.c_int32, vp, C.c_int32, vp, C.c_float]
         L.ariel_ref_set_faithful.argtypes = [vp, C.c_int32]
         L.ariel_ref_set_faithful.restype = None
         L.ariel_ref_set_threads.argtypes = [C.c_int32]
@@ -104,6 +105,12 @@ class RefSim:
             self.close()
         except Exception:
             pass
+
+    def add_mesh(self, vertices, triangles, translate=(0.0, 0.0, 0.0), scale=1.0):
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, np.int32).reshape(-1, 3)
+        tr = np.ascontiguousarray(translate, np.float32).reshape(3)
+        _check(self.L.ariel_ref_add_mesh(self.h, _p(v), len(v), _p(t), len(t), _p(tr), float(scale)), "add_mesh")
 
     def init(self):
         _check(self.L.ariel_ref_init(self.h), "ariel_ref_init")

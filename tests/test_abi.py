@@ -37,7 +37,7 @@ def test_defaults_match_reference_constants():
     L.ariel_scene_dambreak(C.byref(d), 64)
     assert d.dim == 64 and d.density == 0.5 and abs(d.stepsize - 1 / 240) < 1e-9
     assert d.n_forces == 1 and abs(d.forces[0][1] + 9.8) < 1e-6
-    assert L.ariel_abi_version() == 1
+    assert L.ariel_abi_version() == 2
 
 
 def test_status_strings():
@@ -54,3 +54,28 @@ def test_no_device_is_reported_not_faked():
     h = C.c_void_p()
     assert L.ariel_create(C.byref(d), C.byref(p), C.byref(h)) == A.ARIEL_ERR_NO_DEVICE
     assert L.ariel_selftest_barrier_timeout(1.0) == A.ARIEL_ERR_NO_DEVICE
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirror (ariel_b200/_abi.py) against the C compiler's view of include/ariel.h:
+    size of every struct and offset of a few late fields."""
+    import shutil
+    import subprocess
+    structs = ["AsimBox", "AsimSphere", "AsimSceneDesc", "AsimParams", "AsimStats", "AsimSolverTotals",
+               "AsimServerConfig", "AsimRequestInfo", "AsimServerStats"]
+    fields = [("AsimSceneDesc", "seed"), ("AsimSceneDesc", "n_mesh"), ("AsimSceneDesc", "mesh"),
+              ("AsimParams", "sweep_brick"), ("AsimStats", "stage_ms")]
+    src = tmp_path / "sizes.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ariel.h"', "int main(void) {"]
+    lines += ['printf("%s %%zu\\n", sizeof(%s));' % (s, s) for s in structs]
+    lines += ['printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (s, f, s, f) for s, f in fields]
+    lines += ["return 0; }"]
+    src.write_text("\n".join(lines))
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    exe = tmp_path / "sizes"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
+    for s in structs:
+        assert int(out[s]) == C.sizeof(getattr(A, s)), s
+    for s, f in fields:
+        assert int(out["%s.%s" % (s, f)]) == getattr(getattr(A, s), f).offset, (s, f)

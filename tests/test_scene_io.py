@@ -66,8 +66,56 @@ def test_scene_file_refuses_what_it_cannot_represent(tmp_path, bad):
           "grid": dict(dim={"x": 64, "y": 32, "z": 64})}[bad]
     p = tmp_path / "bad.json"
     p.write_text(json.dumps(_scene_json(64, **kw)))
+    # (the "file" case: a liquid read from an OBJ file; only box liquids are seeded)
+    (tmp_path / "tank.obj").write_text(_CUBE_OBJ)
     with pytest.raises(SceneError):
         load_scene(str(p))
+
+
+_CUBE_OBJ = """# unit cube, quads
+v 0 0 0
+v 1 0 0
+v 1 1 0
+v 0 1 0
+v 0 0 1
+v 1 0 1
+v 1 1 1
+v 0 1 1
+f 1 4 3 2
+f 5 6 7 8
+f 1 2 6 5
+f 2 3 7 6
+f 3 4 8 7
+f 4 1 5 8
+"""
+
+
+def test_scene_file_mesh_solids(tmp_path):
+    """A solid read from an OBJ file (translated and scaled) and a box solid become static solid
+    meshes of the scene; the sphere stays analytic."""
+    from ariel_b200.sceneloader import read_obj
+    (tmp_path / "rock.obj").write_text(_CUBE_OBJ)
+    v, t = read_obj(str(tmp_path / "rock.obj"))
+    assert len(v) == 8 and len(t) == 12
+    root = _scene_json(64)
+    root["meshfiles"].append({"id": "rockfile", "file": "rock.obj"})
+    root["meshfiles"].append({"id": "slab", "mesh_gen": "box", "point0": {"x": 40, "y": 0, "z": 10},
+                              "point1": {"x": 50, "y": 8, "z": 20}})
+    root["transforms"].append({"id": "placed", "translation": {"x": 44, "y": 10, "z": 40},
+                               "scale": {"x": 6, "y": 6, "z": 6}})
+    root["geoms"].append({"id": "r2", "type": "mesh", "geom_frames": ["rockfile"], "transform_frames": ["placed"]})
+    root["geoms"].append({"id": "s2", "type": "mesh", "geom_frames": ["slab"], "transform_frames": ["identity"]})
+    root["sim"] += [{"geom": "r2", "type": "solid"}, {"geom": "s2", "type": "solid"}]
+    p = tmp_path / "meshes.json"
+    p.write_text(json.dumps(root))
+    d, info = load_scene(str(p))
+    assert d.n_solid == 1 and d.n_mesh == 2 and len(info["meshes"]) == 2
+    m = info["meshes"][0]
+    assert abs(m.scale - 6.0 / 64) < 1e-7 and abs(float(m.translate[0]) - 44.0 / 64) < 1e-7
+    prm = params(precision=A.PREC_MIXED)
+    base = A.scene_dambreak(64, liquid_hi=(0.4, 0.6, 1.0), dt=1.0 / 480.0, seed=1, jitter=0.0,
+                            spheres=[((0.6, 0.3, 0.5), 0.15)])
+    assert state_bytes([d], prm) > state_bytes([base], prm)  # the meshes' trees and their solids
 
 
 @pytest.mark.gpu
