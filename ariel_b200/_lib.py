@@ -20,6 +20,10 @@ SIGNATURES = {
     "ariel_scene_dambreak": ([C.POINTER(A.AsimSceneDesc), C.c_int32], None),
     "ariel_mesh_create": ([_vp, C.c_int32, _vp, C.c_int32, _vp, C.c_float, C.POINTER(C.c_int32)], C.c_int),
     "ariel_mesh_destroy": ([C.c_int32], C.c_int),
+    "ariel_get_level_set": ([_vp, C.c_int32, _vp, C.c_int64], C.c_int),
+    "ariel_surface_mesh": ([_vp, C.c_int32, _vp, C.c_int64, _vp, C.c_int64, C.POINTER(C.c_int64),
+                            C.POINTER(C.c_int64)], C.c_int),
+    "ariel_export_surface": ([_vp, C.c_int32, C.c_char_p, C.c_int32], C.c_int),
     "ariel_status_string": ([C.c_int], C.c_char_p),
     "ariel_create": ([C.POINTER(A.AsimSceneDesc), C.POINTER(A.AsimParams), C.POINTER(_vp)], C.c_int),
     "ariel_create_batch": ([C.POINTER(A.AsimSceneDesc), C.c_int32, C.POINTER(A.AsimParams), C.POINTER(_vp)], C.c_int),

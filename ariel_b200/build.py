@@ -14,7 +14,7 @@ SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(HERE, "_build")
 SO = os.path.join(OUT_DIR, "libariel_b200.so")
-SOURCES = ["scan.cu", "particles.cu", "grid.cu", "pcg.cu", "host.cu", "server.cu", "noalloc.cu", "mesh.cu"]
+SOURCES = ["scan.cu", "particles.cu", "grid.cu", "pcg.cu", "host.cu", "server.cu", "noalloc.cu", "mesh.cu", "surface.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -69,7 +69,7 @@ def build(verbose=False, extra=()):
             if log.strip():
                 print(log)
     if not os.path.exists(SO) or any(os.path.getmtime(o) > os.path.getmtime(SO) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", host_compiler(), "-o", SO] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", host_compiler(), "-o", SO] + objs + ["-lcudart", "-lz"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stdout + r.stderr))

@@ -19,6 +19,8 @@
 #include <thread>
 #include <vector>
 
+#include <zlib.h>
+
 #include "sim.cuh"
 
 using namespace ariel;
@@ -1598,21 +1600,26 @@ ariel_status ariel_checkpoint_load(ariel_sim* s, const char* path) {
 // ---- particle export (Scene::ExportParticles' Partio branch, src/scene/scene.cpp:35-80) ----
 // FLUID particles in id order with attributes position (grid units: unit position x maxd), v
 // and id (their index in the export), to `path` with the four-digit frame inserted before the
-// extension (".gz" counted as part of it).  Written in Houdini's classic ASCII geometry form
-// (the ".geo" one of Partio's formats); other extensions are refused.
+// extension (".gz" counted as part of it, scene.cpp:52-58).  Written in Houdini's classic ASCII
+// geometry form (the ".geo" one of Partio's formats), gzip-compressed for ".geo.gz"; other
+// extensions are refused.
 ariel_status ariel_export_particles(ariel_sim* s, int32_t scene, const char* path, int32_t frame) {
     if (!s || !path || scene < 0 || scene >= s->k || frame < 0) return ARIEL_ERR_INVALID_ARG;
     std::string name(path);
+    bool gz = false;
+    if (name.size() > 3 && name.compare(name.size() - 3, 3, ".gz") == 0) {
+        gz = true;
+        name = name.substr(0, name.size() - 3);
+    }
     const size_t slash = name.find_last_of('/');
     const size_t dot = name.find_last_of('.');
     if (dot == std::string::npos || (slash != std::string::npos && dot < slash)) return ARIEL_ERR_INVALID_ARG;
     std::string ext = name.substr(dot);
     std::string stem = name.substr(0, dot);
-    if (ext == ".gz") return ARIEL_ERR_INVALID_ARG;  // compressed output is not written
     if (ext != ".geo") return ARIEL_ERR_INVALID_ARG;
     char fr[16];
     std::snprintf(fr, sizeof(fr), ".%04d", frame);
-    const std::string out = stem + fr + ext;
+    const std::string out = stem + fr + ext + (gz ? ".gz" : "");
     const long long b = s->ppref[scene], n = s->ppref[scene + 1] - b;
     std::vector<float4> p4(n), v4(n);
     ARIEL_CUDA(cudaStreamSynchronize(s->stream));
@@ -1624,20 +1631,38 @@ ariel_status ariel_export_particles(ariel_sim* s, int32_t scene, const char* pat
     std::vector<long long> fluid;
     for (long long i = 0; i < n; ++i)
         if (type_bits(v4[i]) == ARIEL_FLUID) fluid.push_back(i);
-    FILE* f = std::fopen(out.c_str(), "w");
-    if (!f) return ARIEL_ERR_INVALID_ARG;
-    std::fprintf(f, "PGEOMETRY V5\nNPoints %lld NPrims 1\nNPointGroups 0 NPrimGroups 0\n", (long long)fluid.size());
-    std::fprintf(f, "NPointAttrib 2 NVertexAttrib 0 NPrimAttrib 0 NAttrib 0\nPointAttrib\n");
-    std::fprintf(f, "v 3 vector 0 0 0\nid 1 int 0\n");
+    std::string text;
+    char line[256];
+    std::snprintf(line, sizeof(line), "PGEOMETRY V5\nNPoints %lld NPrims 1\nNPointGroups 0 NPrimGroups 0\n",
+                  (long long)fluid.size());
+    text += line;
+    text += "NPointAttrib 2 NVertexAttrib 0 NPrimAttrib 0 NAttrib 0\nPointAttrib\n";
+    text += "v 3 vector 0 0 0\nid 1 int 0\n";
     for (size_t e = 0; e < fluid.size(); ++e) {
         const float4& p = p4[fluid[e]];
         const float4& v = v4[fluid[e]];
-        std::fprintf(f, "%.9g %.9g %.9g 1 (%.9g %.9g %.9g %zu)\n", p.x * maxd, p.y * maxd, p.z * maxd, v.x, v.y, v.z, e);
+        std::snprintf(line, sizeof(line), "%.9g %.9g %.9g 1 (%.9g %.9g %.9g %zu)\n", p.x * maxd, p.y * maxd,
+                      p.z * maxd, v.x, v.y, v.z, e);
+        text += line;
     }
-    std::fprintf(f, "Part %lld", (long long)fluid.size());
-    for (size_t e = 0; e < fluid.size(); ++e) std::fprintf(f, " %zu", e);
-    std::fprintf(f, "\nbeginExtra\nendExtra\n");
-    return std::fclose(f) == 0 ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
+    std::snprintf(line, sizeof(line), "Part %lld", (long long)fluid.size());
+    text += line;
+    for (size_t e = 0; e < fluid.size(); ++e) {
+        std::snprintf(line, sizeof(line), " %zu", e);
+        text += line;
+    }
+    text += "\nbeginExtra\nendExtra\n";
+    if (gz) {
+        gzFile f = gzopen(out.c_str(), "wb");
+        if (!f) return ARIEL_ERR_INVALID_ARG;
+        const int wrote = text.empty() ? 0 : gzwrite(f, text.data(), (unsigned)text.size());
+        const int closed = gzclose(f);
+        return (wrote == (int)text.size() && closed == Z_OK) ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
+    }
+    FILE* f = std::fopen(out.c_str(), "w");
+    if (!f) return ARIEL_ERR_INVALID_ARG;
+    const size_t wrote = std::fwrite(text.data(), 1, text.size(), f);
+    return (std::fclose(f) == 0 && wrote == text.size()) ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
 }
 
 int64_t ariel_kernel_launches(void) { return launch_count(); }

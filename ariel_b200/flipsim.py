@@ -161,6 +161,28 @@ class Batch:
         return dict(stage_ms=ms, solve_kernel_ms=solve_k.value, steps=n.value,
                     step_ms=steps[:min(n.value, max_steps)].copy())
 
+    def level_set(self, scene=0):
+        """The liquid surface's level set ((n+5)^3 samples, sample (i,j,k) at grid point
+        (i-2, j-2, k-2))."""
+        N = self.dim(scene) + 5
+        phi = np.zeros((N, N, N), np.float32)
+        check(self.L.ariel_get_level_set(self.h, scene, _p(phi), phi.nbytes), "ariel_get_level_set")
+        return phi
+
+    def surface_mesh(self, scene=0):
+        """(vertices (V,3) in grid units, quads (Q,4) 0-based) of the liquid surface."""
+        nv, nq = C.c_int64(), C.c_int64()
+        check(self.L.ariel_surface_mesh(self.h, scene, None, 0, None, 0, C.byref(nv), C.byref(nq)),
+              "ariel_surface_mesh")
+        v = np.zeros((nv.value, 3), np.float32)
+        q = np.zeros((nq.value, 4), np.int32)
+        check(self.L.ariel_surface_mesh(self.h, scene, _p(v), nv.value, _p(q), nq.value, C.byref(nv), C.byref(nq)),
+              "ariel_surface_mesh")
+        return v, q
+
+    def export_surface(self, path, frame, scene=0):
+        check(self.L.ariel_export_surface(self.h, scene, str(path).encode(), frame), "ariel_export_surface")
+
     def checkpoint_save(self, path):
         check(self.L.ariel_checkpoint_save(self.h, str(path).encode()), "ariel_checkpoint_save")
 
@@ -168,10 +190,13 @@ class Batch:
         check(self.L.ariel_checkpoint_load(self.h, str(path).encode()), "ariel_checkpoint_load")
 
     def export_particles(self, path, frame, scene=0):
-        """Scene::ExportParticles' particle file (Houdini ASCII .geo); returns the written path."""
+        """Scene::ExportParticles' particle file (Houdini ASCII .geo, or .geo.gz); returns the
+        written path."""
         check(self.L.ariel_export_particles(self.h, scene, str(path).encode(), frame), "ariel_export_particles")
-        stem, ext = str(path).rsplit(".", 1)
-        return "%s.%04d.%s" % (stem, frame, ext)
+        p = str(path)
+        gz = p.endswith(".gz")
+        stem, ext = (p[:-3] if gz else p).rsplit(".", 1)
+        return "%s.%04d.%s%s" % (stem, frame, ext, ".gz" if gz else "")
 
     def solver_totals(self, scene=0):
         t = A.AsimSolverTotals()

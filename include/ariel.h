@@ -291,11 +291,33 @@ ariel_status ariel_checkpoint_save(ariel_sim* sim, const char* path);
 ariel_status ariel_checkpoint_load(ariel_sim* sim, const char* path);
 /* Scene::ExportParticles' particle branch (src/scene/scene.cpp:35-80): FLUID particles with
  * position (grid units), v and id, to `path` with ".%04d" of `frame` inserted before the
- * extension.  Written as Houdini classic ASCII geometry; `path` must end in ".geo". */
+ * extension (".gz" counted as part of it).  Written as Houdini classic ASCII geometry; `path`
+ * must end in ".geo", or ".geo.gz" for gzip-compressed output. */
 ariel_status ariel_export_particles(ariel_sim* sim, int32_t scene, const char* path, int32_t frame);
 
 /* Count of this library's kernel launches issued so far (all handles). */
 int64_t ariel_kernel_launches(void);
+
+/* Liquid surface of one scene, for output: the reference's LevelSet(particles) (OpenVDB
+ * ParticlesToLevelSet, src/grid/levelset.cpp:101-111) and LevelSet::WriteObjToFile (OpenVDB
+ * VolumeToMesh, levelset.cpp:113-172), which Scene::ExportParticles' VDB/OBJ branch calls
+ * (src/scene/scene.cpp:84-100).  The level set: FLUID particles as spheres of radius 0.5 cells
+ * rasterised on the integer points of the grid, padded 2 cells beyond each wall; a sample holds
+ * the smallest (distance to a particle - 0.5) within 2 cells, else 1.5.  The mesh: surface nets
+ * at level 0 (one vertex per sign-changing grid cube, one quad per sign-changing grid edge,
+ * normals from inside to outside), in grid units.  Temporaries are allocated for the call.
+ *
+ * ariel_get_level_set: N^3 floats, N = n + 5, sample (i, j, k) at grid point (i-2, j-2, k-2),
+ *   i slowest.
+ * ariel_surface_mesh: the counts, and -- when the buffers are given and large enough --
+ *   vertices (xyz floats) and quads (4 vertex indices each, 0-based).  Buffers too small:
+ *   ARIEL_ERR_INVALID_ARG with the counts set.
+ * ariel_export_surface: the mesh as a Wavefront OBJ at `path` (ending in ".obj") with ".%04d" of
+ *   `frame` inserted before the extension (Scene::ExportParticles' naming, scene.cpp:89-90). */
+ariel_status ariel_get_level_set(ariel_sim* sim, int32_t scene, float* phi, int64_t nbytes);
+ariel_status ariel_surface_mesh(ariel_sim* sim, int32_t scene, float* vertices, int64_t max_vertices, int32_t* quads,
+                                int64_t max_quads, int64_t* n_vertices, int64_t* n_quads);
+ariel_status ariel_export_surface(ariel_sim* sim, int32_t scene, const char* path, int32_t frame);
 
 /* Text of the last CUDA failure seen by this thread (the failing call and CUDA's message). */
 const char* ariel_last_error(void);

@@ -217,7 +217,8 @@ class FlipSim {
     // FlipSim::Step (flip.cpp:92-128).  With any export flag set the particles are written after
     // the step: through the host scene's ExportParticles when constructed from one; otherwise
     // savePARTIO writes ariel_export_particles' Houdini ASCII geometry to the path given by
-    // SetPartioPath, and saveVDB/saveOBJ (OpenVDB surfacing) are refused.
+    // SetPartioPath, saveOBJ the liquid surface (ariel_export_surface) to the path given by
+    // SetMeshPath, and saveVDB (an OpenVDB file) is refused.
     void Step(bool saveVDB = false, bool saveOBJ = false, bool savePARTIO = false) {
         check(ariel_step(sim_, 1), "ariel_step");
         ++m_frame;
@@ -232,15 +233,22 @@ class FlipSim {
             export_(GetParticles(), m_frame, saveVDB, saveOBJ, savePARTIO);
             return;
         }
-        if (saveVDB || saveOBJ)
-            throw Error(ARIEL_ERR_INVALID_ARG, "Step: VDB/OBJ export needs the host scene's writers");
-        if (partio_path_.empty()) throw Error(ARIEL_ERR_INVALID_ARG, "Step: savePARTIO without SetPartioPath");
-        check(ariel_export_particles(sim_, 0, partio_path_.c_str(), m_frame), "ariel_export_particles");
+        if (saveVDB) throw Error(ARIEL_ERR_INVALID_ARG, "Step: VDB export needs the host scene's writers");
+        if (savePARTIO) {
+            if (partio_path_.empty()) throw Error(ARIEL_ERR_INVALID_ARG, "Step: savePARTIO without SetPartioPath");
+            check(ariel_export_particles(sim_, 0, partio_path_.c_str(), m_frame), "ariel_export_particles");
+        }
+        if (saveOBJ) {
+            if (mesh_path_.empty()) throw Error(ARIEL_ERR_INVALID_ARG, "Step: saveOBJ without SetMeshPath");
+            check(ariel_export_surface(sim_, 0, mesh_path_.c_str(), m_frame), "ariel_export_surface");
+        }
     }
 
     // Target of savePARTIO without a host scene (Scene::SetPaths' partio path, scene.cpp:26-33);
     // must end in ".geo", the frame number is inserted before the extension.
     void SetPartioPath(const std::string& path) { partio_path_ = path; }
+    // Target of saveOBJ without a host scene (Scene::SetPaths' mesh path): must end in ".obj".
+    void SetMeshPath(const std::string& path) { mesh_path_ = path; }
 
     // FlipSim::GetParticles (flip.hpp:29): a host copy, refreshed on each call.
     const Particles& GetParticles() {
@@ -279,7 +287,7 @@ class FlipSim {
     bool verbose_;
     ariel_sim* sim_ = nullptr;
     Particles parts_;
-    std::string partio_path_;
+    std::string partio_path_, mesh_path_;
     std::function<void(Particles&)> seed_;
     std::function<void(const Particles&, int, bool, bool, bool)> export_;
 };

@@ -2022,6 +2022,130 @@ ariel_status ariel_ref_apply_fp64(int32_t n, const int32_t* flags, const float* 
     return ARIEL_OK;
 }
 
+// ---- liquid surface (the checker of ariel_get_level_set / ariel_surface_mesh) ----
+// LevelSet(particles) (levelset.cpp:101-111) as spheres of radius 0.5 cells on the integer grid
+// points padded 2 cells beyond the walls, band 1.5 cells, then surface nets at level 0: serial
+// loops over the particles in id order, the cubes and the edges in grid order.
+namespace {
+const int kSPad = 2;
+const float kSRadius = 0.5f, kSBand = 1.5f;
+
+void LevelSetOf(const Sim& s, std::vector<float>& phi, int& N) {
+    N = s.n + 1 + 2 * kSPad;
+    phi.assign((size_t)N * N * N, kSBand);
+    const float maxd = s.maxd;
+    const float R = kSRadius + kSBand, R2 = R * R;
+    for (const Particle& P : s.parts) {
+        if (P.type != ARIEL_FLUID) continue;
+        const float px = P.p.x * maxd, py = P.p.y * maxd, pz = P.p.z * maxd;
+        const float pp[3] = {px, py, pz};
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::max((int)std::ceil(pp[a] - R), -kSPad);
+            hi[a] = std::min((int)std::floor(pp[a] + R), N - 1 - kSPad);
+        }
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+            const float dx = (float)i - px;
+            for (int j = lo[1]; j <= hi[1]; ++j) {
+                const float dy = (float)j - py;
+                for (int k = lo[2]; k <= hi[2]; ++k) {
+                    const float dz = (float)k - pz;
+                    const float d2 = (dx * dx + dy * dy) + dz * dz;
+                    if (!(d2 < R2)) continue;
+                    const float v = std::sqrt(d2) - kSRadius;
+                    float& c = phi[((size_t)(i + kSPad) * N + (j + kSPad)) * N + (k + kSPad)];
+                    if (v < c) c = v;
+                }
+            }
+        }
+    }
+}
+}  // namespace
+
+ariel_status ariel_ref_level_set(ariel_ref* r, float* phi, int64_t nbytes) {
+    if (!r || !phi) return ARIEL_ERR_INVALID_ARG;
+    std::vector<float> ls;
+    int N = 0;
+    LevelSetOf(*r, ls, N);
+    if ((size_t)nbytes != ls.size() * sizeof(float)) return ARIEL_ERR_INVALID_ARG;
+    std::memcpy(phi, ls.data(), (size_t)nbytes);
+    return ARIEL_OK;
+}
+
+ariel_status ariel_ref_surface_mesh(ariel_ref* r, float* vertices, int64_t max_vertices, int32_t* quads,
+                                    int64_t max_quads, int64_t* n_vertices, int64_t* n_quads) {
+    if (!r || !n_vertices || !n_quads) return ARIEL_ERR_INVALID_ARG;
+    std::vector<float> phi;
+    int N = 0;
+    LevelSetOf(*r, phi, N);
+    const int M = N - 1;
+    auto at = [&](int i, int j, int k) { return phi[((size_t)i * N + j) * N + k]; };
+    std::vector<int> vidx((size_t)M * M * M, -1);
+    std::vector<float> V;
+    const int E[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+    for (int i = 0; i < M; ++i)
+        for (int j = 0; j < M; ++j)
+            for (int k = 0; k < M; ++k) {
+                float c[8];
+                int inside = 0;
+                for (int b = 0; b < 8; ++b) {
+                    c[b] = at(i + (b & 1), j + ((b >> 1) & 1), k + ((b >> 2) & 1));
+                    inside += c[b] < 0.0f ? 1 : 0;
+                }
+                if (inside == 0 || inside == 8) continue;
+                float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+                int cnt = 0;
+                for (int e = 0; e < 12; ++e) {
+                    const int a = E[e][0], b = E[e][1];
+                    if ((c[a] < 0.0f) == (c[b] < 0.0f)) continue;
+                    const float t = c[a] / (c[a] - c[b]);
+                    const float ax = (float)(i + (a & 1)), ay = (float)(j + ((a >> 1) & 1)), az = (float)(k + ((a >> 2) & 1));
+                    const int axis = e / 4;
+                    sx += axis == 0 ? ax + t : ax;
+                    sy += axis == 1 ? ay + t : ay;
+                    sz += axis == 2 ? az + t : az;
+                    ++cnt;
+                }
+                const float fc = (float)cnt;
+                vidx[((size_t)i * M + j) * M + k] = (int)(V.size() / 3);
+                V.push_back(sx / fc - (float)kSPad);
+                V.push_back(sy / fc - (float)kSPad);
+                V.push_back(sz / fc - (float)kSPad);
+            }
+    std::vector<int32_t> Q;
+    const int du[4] = {-1, 0, 0, -1}, dw[4] = {-1, -1, 0, 0};
+    for (int axis = 0; axis < 3; ++axis)
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j)
+                for (int k = 0; k < N; ++k) {
+                    const int p[3] = {i, j, k};
+                    if (p[axis] >= N - 1) continue;
+                    const int u = (axis + 1) % 3, w = (axis + 2) % 3;
+                    if (p[u] < 1 || p[u] > N - 2 || p[w] < 1 || p[w] > N - 2) continue;
+                    int q[3] = {i, j, k};
+                    q[axis] += 1;
+                    const float a = at(i, j, k), b = at(q[0], q[1], q[2]);
+                    if ((a < 0.0f) == (b < 0.0f)) continue;
+                    int v[4];
+                    for (int c = 0; c < 4; ++c) {
+                        int rr[3] = {i, j, k};
+                        rr[u] += du[c];
+                        rr[w] += dw[c];
+                        v[c] = vidx[((size_t)rr[0] * M + rr[1]) * M + rr[2]];
+                    }
+                    if (!(a < 0.0f)) {
+                        Q.insert(Q.end(), {v[0], v[3], v[2], v[1]});
+                    } else {
+                        Q.insert(Q.end(), {v[0], v[1], v[2], v[3]});
+                    }
+                }
+    *n_vertices = (int64_t)(V.size() / 3);
+    *n_quads = (int64_t)(Q.size() / 4);
+    if (vertices && *n_vertices <= max_vertices) std::memcpy(vertices, V.data(), V.size() * sizeof(float));
+    if (quads && *n_quads <= max_quads) std::memcpy(quads, Q.data(), Q.size() * sizeof(int32_t));
+    return ARIEL_OK;
+}
+
 void ariel_ref_philox4x32_10(const uint32_t* c, const uint32_t* k, uint32_t* out) {
     u4 in{{c[0], c[1], c[2], c[3]}};
     u4 o = philox(in, k[0], k[1]);

@@ -68,6 +68,12 @@ ariel_status ariel_ref_solve_fp64(int32_t n, const int32_t* flags, const float* 
 ariel_status ariel_ref_apply_fp64(int32_t n, const int32_t* flags, const float* L, const double* x,
                                   double* y);
 
+/* The liquid surface of the oracle's particles: the level set and the surface-nets mesh of
+ * ariel_get_level_set / ariel_surface_mesh (include/ariel.h), computed by serial loops. */
+ariel_status ariel_ref_level_set(ariel_ref* r, float* phi, int64_t nbytes);
+ariel_status ariel_ref_surface_mesh(ariel_ref* r, float* vertices, int64_t max_vertices, int32_t* quads,
+                                    int64_t max_quads, int64_t* n_vertices, int64_t* n_quads);
+
 /* Philox4x32-10 block (counter c[4], key k[2]) -> out[4]; exposed for known-answer tests. */
 void ariel_ref_philox4x32_10(const uint32_t* c, const uint32_t* k, uint32_t* out);
 

@@ -55,6 +55,9 @@ def lib():
         L.ariel_ref_solve_fp64.argtypes = [C.c_int32, vp, vp, vp, vp, C.c_double, C.c_int32,
                                            C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         L.ariel_ref_apply_fp64.argtypes = [C.c_int32, vp, vp, vp, vp]
+        L.ariel_ref_level_set.argtypes = [vp, vp, C.c_int64]
+        L.ariel_ref_surface_mesh.argtypes = [vp, vp, C.c_int64, vp, C.c_int64, C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int64)]
         L.ariel_ref_philox4x32_10.argtypes = [vp, vp, vp]
         L.ariel_ref_philox4x32_10.restype = None
         _lib = L
@@ -170,6 +173,21 @@ class RefSim:
         v = C.c_float()
         _check(self.L.ariel_ref_get_max_density(self.h, C.byref(v)), "max_density")
         return v.value
+
+    def level_set(self):
+        N = self.n + 5
+        phi = np.zeros((N, N, N), np.float32)
+        _check(self.L.ariel_ref_level_set(self.h, _p(phi), phi.nbytes), "level_set")
+        return phi
+
+    def surface_mesh(self):
+        nv, nq = C.c_int64(), C.c_int64()
+        _check(self.L.ariel_ref_surface_mesh(self.h, None, 0, None, 0, C.byref(nv), C.byref(nq)), "surface_mesh")
+        v = np.zeros((nv.value, 3), np.float32)
+        q = np.zeros((nq.value, 4), np.int32)
+        _check(self.L.ariel_ref_surface_mesh(self.h, _p(v), nv.value, _p(q), nq.value, C.byref(nv), C.byref(nq)),
+               "surface_mesh")
+        return v, q
 
     def stage_ms(self):
         a = np.zeros(A.STAGE_COUNT, np.float64)

@@ -165,3 +165,12 @@ def test_particle_export(tmp_path):
     np.testing.assert_array_equal(pos, st["pos"][fl] * np.float32(16))
     np.testing.assert_array_equal(rest[:, :3].astype(np.float32), st["vel"][fl])
     np.testing.assert_array_equal(rest[:, 3], np.arange(fl.sum()))
+    # the same file gzip-compressed for a ".geo.gz" path, frame number before ".geo.gz"
+    import gzip
+    b = Batch([d], params())
+    b.init()
+    b.step(2)
+    gzpath = b.export_particles(tmp_path / "parts.geo.gz", 7)
+    b.close()
+    assert os.path.basename(gzpath) == "parts.0007.geo.gz"
+    assert gzip.open(gzpath, "rt").read().splitlines() == lines
