@@ -790,8 +790,11 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs A) {
                             P.inner_done = 0;
                             P.rr = rr;
                             if (MODE == kMixed) {
+                                // the correction solve stops at the final tolerance itself (its
+                                // fp32 residual); the true fp64 residual then decides whether
+                                // another sweep is needed
                                 double t1 = A.inner_tol * A.inner_tol * rr;
-                                double t2 = A.stop_rule == ARIEL_STOP_REL ? 0.25 * lim2 : 0.0;
+                                double t2 = A.stop_rule == ARIEL_STOP_REL ? lim2 : 0.0;
                                 P.target = t1 > t2 ? t1 : t2;
                             } else {
                                 P.target = A.stop_rule == ARIEL_STOP_REL ? lim2 : abs_eps;
@@ -1719,8 +1722,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_pcg_fast(PcgArgs A) {
             P.inner_done = 0;
             P.rr = rr;
             if (MODE == kMixed) {
+                // the correction solve stops at the final tolerance itself (its fp32 residual);
+                // the true fp64 residual then decides whether another sweep is needed
                 double a = A.inner_tol * A.inner_tol * rr;
-                double b = A.stop_rule == ARIEL_STOP_REL ? 0.25 * lim2 : 0.0;
+                double b = A.stop_rule == ARIEL_STOP_REL ? lim2 : 0.0;
                 P.target = a > b ? a : b;
             } else {
                 P.target = A.stop_rule == ARIEL_STOP_REL ? lim2 : abs_eps;

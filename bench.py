@@ -354,6 +354,19 @@ def reference_arm(args, A, ws, rank):
     return 0
 
 
+def mic0_subresult(A, Batch, desc, args):
+    """The same workload with the MIC(0) preconditioner (tau 0.97, FP64 factorisation, brick
+    wavefront sweeps) in MIXED precision: a few graph-replayed steps."""
+    prm = make_params(A, A.PREC_MIXED, args.tol)
+    prm.precond = A.PRECOND_MIC0
+    b, r = run_gpu_pass(A, Batch, desc, prm, args.mic0_steps, 3)
+    t = r["totals"]
+    b.close()
+    return {"ms_per_solve": r["timing"]["solve_kernel_ms"] / max(t.solves, 1),
+            "iterations_per_solve": t.iterations / max(t.solves, 1), "outer_per_solve": t.outer / max(t.solves, 1),
+            "not_converged": t.not_converged, "frames": [4, 3 + args.mic0_steps]}
+
+
 def batch_subresult(A, Batch, args):
     """BASELINE config 4 beside the headline: the uneven 64-scene batch, MIXED against the plain
     FP64 path, a few graph-replayed steps each (step and solve ratios)."""
@@ -492,6 +505,8 @@ def main():
     ap.add_argument("--batch-sub", type=int, default=64,
                     help="dambreak: also time this many uneven scenes batched (config 4), MIXED and FP64; 0: off")
     ap.add_argument("--batch-steps", type=int, default=6)
+    ap.add_argument("--mic0-steps", type=int, default=3,
+                    help="dambreak: also time this many steps with the MIC(0) preconditioner; 0: off")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: mean arrivals per second")
     ap.add_argument("--duration", type=float, default=120.0, help="serve: seconds of arrivals")
@@ -679,6 +694,8 @@ def main():
                                              "(%d iterations), %.1f s" % (args.n, n, args.tol, st.pcg_iterations, dt)}
     if rank == 0 and ws == 1 and args.batch_sub > 0 and args.workload == "dambreak":
         out["batch"] = batch_subresult(A, Batch, args)
+    if rank == 0 and ws == 1 and args.mic0_steps > 0 and args.workload == "dambreak" and PRECOND != "mic0":
+        out["pcg"]["mic0"] = mic0_subresult(A, Batch, desc, args)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if pg:

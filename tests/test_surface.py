@@ -17,16 +17,19 @@ from oracle.pyoracle import RefSim
 from helpers import assert_bits, dambreak, params
 
 
-def _closed_and_volume(v, q):
-    """Every edge of the quad mesh is used once in each direction (closed, consistently wound);
-    returns the enclosed volume (divergence theorem over the quads split in two triangles)."""
+def _closed_and_volume(v, q, manifold=False):
+    """The quad mesh has no boundary: every edge is walked as often in one direction as in the
+    other (closed and consistently wound; where two sheets of the surface touch, surface nets
+    shares an edge among four quads).  With `manifold`, exactly once each way.  Returns the
+    enclosed volume (divergence theorem over the quads split in two triangles)."""
     from collections import Counter
     edges = Counter()
     for a, b, c, d in q:
         for x, y in ((a, b), (b, c), (c, d), (d, a)):
             edges[(x, y)] += 1
     for (x, y), cnt in edges.items():
-        assert cnt == 1 and edges.get((y, x), 0) == 1, "open or inconsistently wound edge %s" % ((x, y),)
+        assert edges.get((y, x), 0) == cnt, "open or inconsistently wound edge %s" % ((x, y),)
+        assert not manifold or cnt == 1, "edge %s shared by more than two quads" % ((x, y),)
     v = v.astype(np.float64)
     tri = np.concatenate([q[:, [0, 1, 2]], q[:, [0, 2, 3]]])
     a, b, c = v[tri[:, 0]], v[tri[:, 1]], v[tri[:, 2]]
@@ -42,7 +45,7 @@ def test_oracle_surface_of_a_block():
     g = lambda x, y, z: phi[x + 2, y + 2, z + 2]
     assert g(3, 4, 8) < 0 and g(12, 14, 8) > 0  # inside the block / in the air
     v, q = r.surface_mesh()
-    vol = _closed_and_volume(v, q)
+    vol = _closed_and_volume(v, q, manifold=True)
     p = r.get_particles()["pos"] * n
     inner = np.prod(p.max(0) - p.min(0))        # the box of the particle centres
     outer = np.prod(p.max(0) - p.min(0) + 1.0)  # the spheres' union reaches 0.5 beyond them
