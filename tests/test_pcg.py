@@ -173,6 +173,27 @@ def test_solve_independent_of_grid_size(precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n,small_grid", [(64, 64), (128, 148)])
+def test_bench_size_solve_independent_of_grid_size(n, small_grid):
+    """At the bench sizes every block of the default grid owns one FLUID chunk and keeps its
+    records in shared memory; on a grid smaller than the chunk count most chunks stream their
+    records through the prefetch pipeline instead.  Both give the same bits, step after step,
+    with the bench's solver settings (MIXED to 1e-5 relative)."""
+    runs = []
+    for nb in (0, small_grid):
+        b = Batch([A.scene_dambreak(n, seed=1)],
+                  params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, pcg_grid_blocks=nb))
+        b.init()
+        b.step(3)
+        runs.append((b.get_particles(0), b.stats(0).pcg_iterations, b.stats(0).pcg_outer))
+        b.close()
+    (p0, it0, o0), (p1, it1, o1) = runs
+    assert (it0, o0) == (it1, o1)
+    for key in ("pos", "vel"):
+        assert np.array_equal(p0[key].view(np.uint8), p1[key].view(np.uint8)), key
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
 def test_batch_solve_independent_of_grid_size(precision):
     """A batch of uneven scenes solved by 1 or 3 blocks steps to the same bits as with the default
