@@ -52,6 +52,8 @@ struct SceneDev {
     float dens_inv_hh;
     int re_pow2;         // resample_re^2 is a power of two
     float re_inv_hh;
+    // reciprocals of the grid's index divisors (n, n + 1, n^2, n (n + 1)) for index decoding
+    double inv_n, inv_n1, inv_nn, inv_nn1;
     // static solid meshes: the scene's tree and triangles (mesh.cuh), world coordinates
     int n_meshes;
     const struct MeshNode* mesh_nodes;
@@ -129,6 +131,46 @@ __host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, ui
 }
 constexpr uint32_t kTagSeed = 0x53454544u;      // "SEED"
 constexpr uint32_t kTagResample = 0x5245534Du;  // "RESM"
+
+// ------------------------------------------------------------------------------------------
+// Grid index decoding without integer division (a 64-bit division is a long instruction
+// sequence, several per thread in the stencil kernels).  floor(x / d) for 0 <= x < 2^40 from a
+// double reciprocal r of d accurate to a few ulp: x * r is then within 2^-11 of the quotient,
+// so its truncation is off by at most one, which the remainder test corrects.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ long long div_r(long long x, long long d, double r) {
+    long long q = (long long)((double)x * r);
+    const long long rem = x - q * d;
+    q += rem < 0 ? -1 : (rem >= d ? 1 : 0);
+    return q;
+}
+// Cell (i, j, k) of local cell index c = (i n + j) n + k.
+__device__ __forceinline__ void cell_ijk(const SceneDev& D, long long c, int& i, int& j, int& k) {
+    const long long n = D.n, nn = n * n;
+    const long long a = div_r(c, nn, D.inv_nn);
+    const long long r = c - a * nn;
+    const long long b = div_r(r, n, D.inv_n);
+    i = (int)a;
+    j = (int)b;
+    k = (int)(r - b * n);
+}
+// Axis and (i, j, k) of local face index f: x faces (n+1) x n x n, then y faces n x (n+1) x n,
+// then z faces n x n x (n+1), each block in (i, j, k) order.
+__device__ __forceinline__ void face_ijk(const SceneDev& D, long long f, int& axis, int& i, int& j, int& k) {
+    const long long n = D.n, n1 = n + 1, per = n * n * n1;
+    axis = (f >= per ? 1 : 0) + (f >= 2 * per ? 1 : 0);
+    const long long r = f - axis * per;
+    const long long rowd = axis == 0 ? n * n : n1 * n;  // faces per i plane
+    const double rowr = axis == 0 ? D.inv_nn : D.inv_nn1;
+    const long long kd = axis == 2 ? n1 : n;            // faces per (i, j) row
+    const double kr = axis == 2 ? D.inv_n1 : D.inv_n;
+    const long long a = div_r(r, rowd, rowr);
+    const long long r2 = r - a * rowd;
+    const long long b = div_r(r2, kd, kr);
+    i = (int)a;
+    j = (int)b;
+    k = (int)(r2 - b * kd);
+}
 
 // ------------------------------------------------------------------------------------------
 // Packed index -> scene.  `pref` holds k+1 ascending begins; a block copies it to shared

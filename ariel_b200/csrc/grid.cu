@@ -32,11 +32,6 @@ struct FaceIdx {
     }
 };
 
-__device__ __forceinline__ void decode_cell(long long local, int n, int& i, int& j, int& k) {
-    i = (int)(local / ((long long)n * n));
-    j = (int)((local / n) % n);
-    k = (int)(local % n);
-}
 
 // ------------------------------------------------------------------------------------------
 __global__ void k_classify(DevState S) {
@@ -79,7 +74,7 @@ __global__ void k_boundary_div(DevState S) {
     const SceneDev& D = S.scenes[find_scene(pref_s, S.k, c)];
     const int n = D.n;
     int i, j, k;
-    decode_cell(c - D.c_begin, n, i, j, k);
+    cell_ijk(D, c - D.c_begin, i, j, k);
     FaceIdx F{D.f_begin, (long long)n * n * (n + 1), n};
     const uint8_t* A = S.flags;
     const long long cb = D.c_begin;
@@ -134,25 +129,6 @@ __global__ void k_boundary_div(DevState S) {
 }
 
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ void face_decode(long long f, int n, int& axis, int& i, int& j, int& k) {
-    const long long per = (long long)n * n * (n + 1);
-    axis = (int)(f / per);
-    long long rem = f - axis * per;
-    if (axis == 0) {
-        i = (int)(rem / ((long long)n * n));
-        j = (int)((rem / n) % n);
-        k = (int)(rem % n);
-    } else if (axis == 1) {
-        i = (int)(rem / ((long long)(n + 1) * n));
-        j = (int)((rem / n) % (n + 1));
-        k = (int)(rem % n);
-    } else {
-        i = (int)(rem / ((long long)n * (n + 1)));
-        j = (int)((rem / (n + 1)) % n);
-        k = (int)(rem % (n + 1));
-    }
-}
-
 __global__ void k_gradient(DevState S) {
     SCENE_PREFIX(S.f_pref);
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,7 +136,7 @@ __global__ void k_gradient(DevState S) {
     const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
     const int n = D.n;
     int axis, i, j, k;
-    face_decode(g - D.f_begin, n, axis, i, j, k);
+    face_ijk(D, g - D.f_begin, axis, i, j, k);
     const long long cb = D.c_begin;
     const int di = axis == 0, dj = axis == 1, dk = axis == 2;
     const int m = axis == 0 ? i : (axis == 1 ? j : k);
@@ -192,7 +168,7 @@ __global__ void k_extrapolate(DevState S) {
     const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
     const int n = D.n;
     int axis, i, j, k;
-    face_decode(g - D.f_begin, n, axis, i, j, k);
+    face_ijk(D, g - D.f_begin, axis, i, j, k);
     const long long cb = D.c_begin;
     const uint8_t* A = S.flags;
     const int di = axis == 0, dj = axis == 1, dk = axis == 2;

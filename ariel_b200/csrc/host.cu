@@ -435,6 +435,11 @@ SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
         *inv = 1.0f / v;
         return (m == 0.5f && std::isfinite(*inv) && *inv * v == 1.0f) ? 1 : 0;
     };
+    const double dn = (double)d.dim;
+    D.inv_n = 1.0 / dn;
+    D.inv_n1 = 1.0 / (dn + 1.0);
+    D.inv_nn = 1.0 / (dn * dn);
+    D.inv_nn1 = 1.0 / (dn * (dn + 1.0));
     D.dens_pow2 = pow2(D.dens_h * D.dens_h, &D.dens_inv_hh);
     D.re_pow2 = pow2(D.resample_re * D.resample_re, &D.re_inv_hh);
     return D;

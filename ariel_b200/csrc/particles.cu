@@ -339,24 +339,8 @@ __global__ void k_p2g(DevState S) {
     int sc = find_scene(pref_s, S.k, g);
     const SceneDev& D = S.scenes[sc];
     const int n = D.n;
-    const long long per = (long long)n * n * (n + 1);
-    long long f = g - D.f_begin;
-    int axis = (int)(f / per);
-    long long rem = f - axis * per;
-    int i, j, k;
-    if (axis == 0) {
-        i = (int)(rem / ((long long)n * n));
-        j = (int)((rem / n) % n);
-        k = (int)(rem % n);
-    } else if (axis == 1) {
-        i = (int)(rem / ((long long)(n + 1) * n));
-        j = (int)((rem / n) % (n + 1));
-        k = (int)(rem % n);
-    } else {
-        i = (int)(rem / ((long long)n * (n + 1)));
-        j = (int)((rem / (n + 1)) % n);
-        k = (int)(rem % (n + 1));
-    }
+    int axis, i, j, k;
+    face_ijk(D, g - D.f_begin, axis, i, j, k);
     // face centre and GetWallNeighbors block [index - nn, index + nn - 1]
     float fx, fy, fz;
     int xlo, xhi, ylo, yhi, zlo, zhi;

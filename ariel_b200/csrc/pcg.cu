@@ -162,12 +162,6 @@ struct VT<kFp64> {
     using T = double;
 };
 
-__device__ __forceinline__ void cell_ijk(long long local, int n, int& i, int& j, int& k) {
-    i = (int)(local / ((long long)n * n));
-    j = (int)((local / n) % n);
-    k = (int)(local % n);
-}
-
 // ------------------------------------------------------------------------------------------
 // Preparation: per-cell operator data, order-free preconditioner, FLUID predicate.
 // ------------------------------------------------------------------------------------------
@@ -192,7 +186,7 @@ __global__ void k_prep_cells(PcgArgs A, uint32_t* pred) {
         return;
     }
     int i, j, k;
-    cell_ijk(c - D.c_begin, n, i, j, k);
+    cell_ijk(D, c - D.c_begin, i, j, k);
     const int q[6][3] = {{i - 1, j, k}, {i + 1, j, k}, {i, j - 1, k}, {i, j + 1, k}, {i, j, k - 1}, {i, j, k + 1}};
     const float Lc = S.L[c];
     float d32 = 6.0f;
@@ -620,7 +614,7 @@ template <class SV>
 __device__ __forceinline__ float ax_ref32(const DevState& S, const SceneDev& D, long long c, float xc, SV&& sv) {
     const int n = D.n;
     int i, j, k;
-    cell_ijk(c - D.c_begin, n, i, j, k);
+    cell_ijk(D, c - D.c_begin, i, j, k);
     const float Lc = S.L[c];
     auto xref = [&](int pi, int pj, int pk) -> float {
         int a = min(max(0, pi), n - 1), b = min(max(0, pj), n - 1), cc = min(max(0, pk), n - 1);
