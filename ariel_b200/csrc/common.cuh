@@ -78,6 +78,16 @@ __device__ __forceinline__ float sqrlength(float ax, float ay, float az, float b
     float c = az - bz;
     return a * a + b * b + c * c;
 }
+// sqrlength(q.x, q.y, q.z, p.x, p.y, p.z) with the x and y terms as one packed pair of IEEE
+// round-to-nearest operations (sm_100 f32x2 add and multiply, each lane the same bits as the
+// scalar operation); `nxy` holds (-p.x, -p.y), and q.x + (-p.x) is q.x - p.x exactly.  The
+// square of a difference does not depend on its sign, so it also serves (p - q) . (p - q).
+__device__ __forceinline__ float sqrlength_xy2(float4 q, float2 nxy, float pz) {
+    const float2 d = __fadd2_rn(make_float2(q.x, q.y), nxy);
+    const float2 s = __fmul2_rn(d, d);
+    const float c = q.z - pz;
+    return s.x + s.y + c * c;
+}
 __device__ __forceinline__ float smooth_k(float r2, float h) { return gmax(1.0f - r2 / (h * h), 0.0f); }
 // smooth_k with the division replaced by an exact power-of-two reciprocal when pow2 is set.
 __device__ __forceinline__ float smooth_fast(float r2, float h, int pow2, float inv_hh) {

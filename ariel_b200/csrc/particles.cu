@@ -259,10 +259,11 @@ __global__ void k_sort_permute(DevState S) {
 template <bool POW2>
 __device__ __forceinline__ float density_run(const float4* __restrict__ sp, uint32_t a, uint32_t b, float px,
                                              float py, float pz, float hk, float inv_hh, float weightsum) {
+    const float2 nxy = make_float2(-px, -py);
 #pragma unroll 4
     for (uint32_t t = a; t < b; ++t) {
         const float4 q = sp[t];
-        const float sqd = sqrlength(q.x, q.y, q.z, px, py, pz);
+        const float sqd = sqrlength_xy2(q, nxy, pz);
         const float weight = q.w * (POW2 ? gmax(1.0f - sqd * inv_hh, 0.0f) : smooth_k(sqd, hk));
         weightsum = weightsum + weight;
     }
@@ -363,6 +364,7 @@ __global__ void k_p2g(DevState S) {
     // rounding) hold only particles whose weight is exactly 0; skipping them leaves the
     // contributing particles in the reference's order.
     const float LIM = 1.1f * RE2;
+    const float2 nfxy = make_float2(-fx, -fy);
     float sumw = 0.0f, sumu = 0.0f;
     if (zlo <= zhi) {
         for (int sx = xlo; sx <= xhi; ++sx) {
@@ -379,7 +381,7 @@ __global__ void k_p2g(DevState S) {
                 uint32_t a = S.start[cb + z0], b = S.start[cb + z1 + 1];
                 for (uint32_t t = a; t < b; ++t) {
                     float4 q = S.gpos4[t];
-                    float r2 = sqrlength(q.x, q.y, q.z, fx, fy, fz);
+                    float r2 = sqrlength_xy2(q, nfxy, fz);
                     // Sharpen is exactly 0 for r2 >= RE^2 (and non-FLUID records are far away)
                     if (!(r2 < RE2)) continue;
                     float4 v = S.svel4[t];
@@ -614,6 +616,7 @@ __global__ void __launch_bounds__(kBlock, 5) k_resample_spring(DevState S) {
         axis_cells(p4.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
     }
     int nl = 0;
+    const float2 npxy = make_float2(-p4.x, -p4.y);
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
             for (int sy = yl; sy <= yh; ++sy) {
@@ -627,9 +630,8 @@ __global__ void __launch_bounds__(kBlock, 5) k_resample_spring(DevState S) {
 #pragma unroll 4
                     for (; t < e; ++t) {
                         const float4 q = S.spos4[t];
-                        const float3 d = make_float3(p4.x - q.x, p4.y - q.y, p4.z - q.z);
                         lst[nl][me] = t;
-                        nl += gdot3(d, d) < near2 ? 1 : 0;
+                        nl += sqrlength_xy2(q, npxy, p4.z) < near2 ? 1 : 0;
                     }
                     if (nl == kResList) {
                         for (int i = 0; i < nl; ++i) eval(lst[i][me]);
@@ -690,6 +692,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
         axis_cells(t.z, min((int)gz, n - 1), n, ch, lim, zl, zh);
     }
     int nl = 0;
+    const float2 ntxy = make_float2(-t.x, -t.y);
     if (zl <= zh) {
         for (int sx = xl; sx <= xh; ++sx)
             for (int sy = yl; sy <= yh; ++sy) {
@@ -704,7 +707,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
                     for (; q < e; ++q) {
                         const float4 np = S.spos4[q];
                         lst[nl][me] = q;
-                        nl += sqrlength(t.x, t.y, t.z, np.x, np.y, np.z) < re2 ? 1 : 0;
+                        nl += sqrlength_xy2(np, ntxy, t.z) < re2 ? 1 : 0;
                     }
                     if (nl == kResList) {
                         for (int i = 0; i < nl; ++i) eval(lst[i][me]);
