@@ -368,8 +368,9 @@ def mic0_subresult(A, Batch, desc, args):
 
 
 def batch_subresult(A, Batch, args):
-    """BASELINE config 4 beside the headline: the uneven 64-scene batch, MIXED against the plain
-    FP64 path, a few graph-replayed steps each (step and solve ratios)."""
+    """The batched workload beside the headline: 64 uneven dam-break scenes (grids drawn from
+    {32,48,64,96,128}^3), MIXED against the plain FP64 path, a few graph-replayed steps each (step
+    and solve ratios)."""
     from ariel_b200 import workloads as W
     descs = W.uneven_batch(args.batch_sub, seed=args.seed)
     res = {}
@@ -503,7 +504,7 @@ def main():
                          "uneven scenes stepped together; serve: Poisson arrivals through the request server")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--batch-sub", type=int, default=64,
-                    help="dambreak: also time this many uneven scenes batched (config 4), MIXED and FP64; 0: off")
+                    help="dambreak: also time this many uneven scenes batched, MIXED and FP64; 0: off")
     ap.add_argument("--batch-steps", type=int, default=6)
     ap.add_argument("--mic0-steps", type=int, default=3,
                     help="dambreak: also time this many steps with the MIC(0) preconditioner; 0: off")

@@ -44,7 +44,7 @@ from oracle.pyoracle import RefSim  # noqa: E402
 CASES = {
     # 16^3 dam break, evolved 5 steps from Init
     "dambreak16": dict(n=16, seed=5, hi=(0.4, 0.6, 1.0), spheres=(), dt=1.0 / 240.0, steps=5),
-    # 16^3 block beside a static solid sphere, dt 1/480 (BASELINE config 3's shape), evolved 4 steps
+    # 16^3 block beside a static solid sphere, dt 1/480 (the 256^3 sphere scene's shape), evolved 4 steps
     "sphere16": dict(n=16, seed=7, hi=(0.35, 0.5, 1.0), spheres=(((0.6, 0.3, 0.5), 0.15),), dt=1.0 / 480.0,
                      steps=4),
 }

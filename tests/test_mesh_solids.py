@@ -1,4 +1,4 @@
-"""Static solid meshes (SURVEY f3: the reference's mesh solids, src/scene/scene.cpp:362-434 and
+"""Static solid meshes (the reference's mesh solids, src/scene/scene.cpp:362-434 and
 src/spatial/bvh.inl, generalising the analytic spheres of the solid constraints).
 
 The CUDA library places every mesh of a scene in one bounding volume hierarchy; the oracle loops

@@ -2,10 +2,10 @@
 
 The stage-by-stage comparison of tests/test_parity_stages.py, run where the size-dependent paths
 of the CUDA library engage:
-  * the 64^3 dam break of BASELINE config 1 (502,656 particles) straight from Init and after ten
+  * the 64^3 dam break (502,656 particles) straight from Init and after ten
     oracle steps, and one whole step from Init;
-  * the 128^3 dam break of config 2 (4,021,248 particles) from Init;
-  * config 3's shape -- liquid beside a static solid sphere c = (.6,.3,.5), r = .15, dt = 1/480,
+  * the 128^3 dam break (4,021,248 particles) from Init;
+  * the sphere scene's shape -- liquid beside a static solid sphere c = (.6,.3,.5), r = .15, dt = 1/480,
     resampling every 5th step -- at 64^3, evolved to frame 4 and compared across a resampling
     step;
   * the pressure solve's streamed chunks (each persistent block holds only its first chunk's

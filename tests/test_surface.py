@@ -1,4 +1,4 @@
-"""Liquid surface for output (SURVEY f4: the reference's particle level set and its mesh,
+"""Liquid surface for output (the reference's particle level set and its mesh,
 src/grid/levelset.cpp:101-172 through OpenVDB, called by Scene::ExportParticles).
 
 The CUDA library rasterises the FLUID particles as spheres of radius 0.5 cells into a level set
