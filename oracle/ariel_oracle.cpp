@@ -1799,6 +1799,21 @@ ariel_status ariel_ref_create(const AsimSceneDesc* desc, const AsimParams* param
 
 void ariel_ref_destroy(ariel_ref* r) { delete r; }
 
+int32_t ariel_ref_tri_ray(const float* v, const float* o, const float* d, float* point) {
+    MTri T{};
+    T.a = mk(v[0], v[1], v[2]);
+    T.b = mk(v[3], v[4], v[5]);
+    T.c = mk(v[6], v[7], v[8]);
+    const vec3 ro = mk(o[0], o[1], o[2]), rd = mk(d[0], d[1], d[2]);
+    float t = 0.0f;
+    if (!TriRay(T, ro, rd, t)) return 0;
+    const vec3 pt = ro + rd * t;
+    point[0] = pt.x;
+    point[1] = pt.y;
+    point[2] = pt.z;
+    return 1;
+}
+
 ariel_status ariel_ref_add_mesh(ariel_ref* r, const float* vertices, int32_t n_vertices, const int32_t* triangles,
                                 int32_t n_triangles, const float* translate, float scale) {
     if (!r || !vertices || !triangles || !translate || n_vertices < 3 || n_triangles < 1 || r->inited)

@@ -33,6 +33,9 @@ void ariel_ref_destroy(ariel_ref* r);
  * translate in the unit cube, after the scene's spheres; queried by brute force. */
 ariel_status ariel_ref_add_mesh(ariel_ref* r, const float* vertices, int32_t n_vertices, const int32_t* triangles,
                                 int32_t n_triangles, const float* translate, float scale);
+/* The mesh queries' ray-triangle test for one triangle v[0..8] and ray (o, d): 1 on a hit, with
+ * the hit point o + d t in point[0..2] (the value the nearest-hit query records). */
+int32_t ariel_ref_tri_ray(const float* v, const float* o, const float* d, float* point);
 /* 1: the reference's own parallel granularity (one parallel region per (j,k) line in Op,
  *    the S copy and the backward sweep, serial Sort and Product) -- the timed CPU baseline.
  * 0: one parallel region per loop nest (same results, faster; used by the tests). */

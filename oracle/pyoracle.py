@@ -34,6 +34,8 @@ def lib():
         L.ariel_ref_destroy.argtypes = [vp]
         L.ariel_ref_destroy.restype = None
         L.ariel_ref_add_mesh.argtypes = [vp, vp, C.c_int32, vp, C.c_int32, vp, C.c_float]
+        L.ariel_ref_tri_ray.argtypes = [vp, vp, vp, vp]
+        L.ariel_ref_tri_ray.restype = C.c_int32
         L.ariel_ref_set_faithful.argtypes = [vp, C.c_int32]
         L.ariel_ref_set_faithful.restype = None
         L.ariel_ref_set_threads.argtypes = [C.c_int32]
@@ -214,6 +216,17 @@ def apply_fp64(n, flags, L, x):
     y = np.zeros(n ** 3, np.float64)
     _check(lib().ariel_ref_apply_fp64(n, _p(flags), _p(L), _p(x), _p(y)), "apply_fp64")
     return y.reshape(n, n, n)
+
+
+def tri_ray(v, o, d):
+    """The mesh queries' ray-triangle test: (hit, hit point o + d t) for the triangle v (3x3)."""
+    import numpy as np
+    v = np.ascontiguousarray(v, np.float32).ravel()
+    o = np.ascontiguousarray(o, np.float32)
+    d = np.ascontiguousarray(d, np.float32)
+    pt = np.zeros(3, np.float32)
+    hit = lib().ariel_ref_tri_ray(_p(v), _p(o), _p(d), _p(pt))
+    return bool(hit), pt
 
 
 def philox(counter, key):

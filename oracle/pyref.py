@@ -20,6 +20,8 @@ _SO = {
     "glm096": os.path.join(_HERE, "_ref", "libariel_reference_glm096.so"),
     # TBB's parallel_for spread over OpenMP threads: the benchmark's CPU reference arm (timed only)
     "omp": os.path.join(_HERE, "_ref", "libariel_reference_omp.so"),
+    # the reference's mesh sources (oracle/ref_mesh_driver.cpp): its ray-triangle test
+    "mesh": os.path.join(_HERE, "_ref", "libariel_reference_mesh.so"),
 }
 _libs = {}
 
@@ -191,6 +193,24 @@ def philox(counter, key, variant="default"):
     o = np.zeros(4, np.uint32)
     lib(variant).ariel_pin_philox4x32_10(_p(c), _p(k), _p(o))
     return o
+
+
+def ray_triangle(v, o, d):
+    """Obj::RayTriangleTest (src/geom/obj/obj.cpp:354-398) of the reference's own build:
+    (hit, hit point) for the triangle v (3x3) and the ray (o, d)."""
+    if "mesh" not in _libs:
+        if not available("mesh"):
+            raise RuntimeError("the reference's sources are not here and oracle/_ref is not built")
+        L = C.CDLL(_SO["mesh"])
+        L.ariel_pin_ray_triangle.argtypes = [C.c_void_p] * 4
+        L.ariel_pin_ray_triangle.restype = C.c_int32
+        _libs["mesh"] = L
+    v = np.ascontiguousarray(v, np.float32).ravel()
+    o = np.ascontiguousarray(o, np.float32)
+    d = np.ascontiguousarray(d, np.float32)
+    pt = np.zeros(3, np.float32)
+    hit = _libs["mesh"].ariel_pin_ray_triangle(_p(v), _p(o), _p(d), _p(pt))
+    return bool(hit), pt
 
 
 def reference_params():

@@ -6,8 +6,9 @@
 //  * UTILITIES_H (src/utilities/utilities.h): the Takua string/matrix helpers.  The FLIP step
 //    uses none of them; only the HOST/DEVICE macros and the glm include are kept.
 //  * RAY_HPP (src/ray/ray.hpp): rayCore::Ray and rayCore::Intersection with the fields the
-//    step reads, the default contents that src/ray/ray.cpp:15-17 and :56-58 give them, and
-//    Intersection::CompareClosestAgainst as src/ray/ray.cpp:83-98 defines it.
+//    step reads, the default contents that src/ray/ray.cpp:15-17 and :56-58 give them,
+//    Intersection::CompareClosestAgainst as src/ray/ray.cpp:83-98 defines it, and (for the
+//    mesh sources) Ray::GetPointAlongRay and the full Intersection constructor of ray.cpp.
 //  * LEVELSET_HPP (src/grid/levelset.hpp): the OpenVDB level set.  Only
 //    ProjectPointsToSurface and GetCell are called by the step; the driver implements them on
 //    analytic spheres.
@@ -44,6 +45,8 @@ namespace rayCore {
 class Ray {
   public:
     Ray() : m_origin(0.0f), m_direction(0.0f, 1.0f, 0.0f), m_trackingID(0), m_frame(0.0f) {}
+    // src/ray/ray.cpp:40-42
+    glm::vec3 GetPointAlongRay(const float& distance) const { return m_origin + distance * m_direction; }
     glm::vec3 m_origin;
     glm::vec3 m_direction;
     unsigned int m_trackingID;
@@ -56,6 +59,10 @@ class Intersection {
         : m_point(0.0f), m_normal(1.0f, 0.0f, 0.0f), m_uv(0.0f), m_objectID(0), m_primID(0), m_hit(false) {}
     Intersection(bool hit, const glm::vec3& point, const glm::vec3& normal)
         : m_point(point), m_normal(normal), m_uv(0.0f), m_objectID(0), m_primID(0), m_hit(hit) {}
+    // src/ray/ray.cpp:60-64
+    Intersection(const bool& hit, const glm::vec3& point, const glm::vec3& normal, const glm::vec2& uv,
+                 const unsigned int& objectID, const unsigned int& primID)
+        : m_point(point), m_normal(normal), m_uv(uv), m_objectID(objectID), m_primID(primID), m_hit(hit) {}
     Intersection CompareClosestAgainst(const Intersection& b, const glm::vec3& point) const {
         if (m_hit && !b.m_hit) return *this;
         if (!m_hit && b.m_hit) return b;

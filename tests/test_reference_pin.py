@@ -163,3 +163,54 @@ def test_rand_stand_in_serves_the_oracle_stream():
     # Salmon et al.'s published known answer for a zero counter and key
     z = pyref.philox(np.zeros(4, np.uint32), np.zeros(2, np.uint32))
     assert [int(v) for v in z] == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+
+
+def _ray_triangle_cases(rng):
+    """Triangles and rays for the mesh queries' ray-triangle test: rays aimed at random points,
+    vertices and edge midpoints of random triangles (grid units), random rays, the +z rays of
+    the inside test against axis-aligned faces (rays in the triangle's plane included), rays hitting
+    from behind, and degenerate triangles."""
+    cases = []
+    for _ in range(3000):
+        v = rng.uniform(0.0, 64.0, (3, 3)).astype(np.float32)
+        o = rng.uniform(-8.0, 72.0, 3).astype(np.float32)
+        w = rng.dirichlet((1.0, 1.0, 1.0))
+        targets = [w @ v, v[0], v[1], v[2], 0.5 * (v[0] + v[1]), 0.5 * (v[1] + v[2])]
+        for tgt in targets:
+            d = (np.asarray(tgt, np.float64) - o).astype(np.float32)
+            n = np.sqrt(np.float32(np.dot(d, d)))
+            if n > 0:
+                cases.append((v, o, (d / n).astype(np.float32)))
+        d = rng.normal(size=3).astype(np.float32)
+        cases.append((v, o, (d / np.sqrt(np.dot(d, d))).astype(np.float32)))
+        cases.append((v, o, -cases[-2][2]))  # the aimed ray reversed: a hit behind the origin
+    z = np.array([0.0, 0.0, 1.0], np.float32)
+    for _ in range(2000):
+        a, b = sorted(rng.integers(0, 32, 2))
+        c = rng.integers(0, 32)
+        quad = np.array([[a, a, c], [b, a, c], [b, b, c]], np.float32)  # a face normal to z
+        side = np.array([[a, c, a], [b, c, a], [b, c, b]], np.float32)  # a face containing z
+        o = np.array([rng.integers(0, 32) + 0.5, rng.integers(0, 32) + 0.5, rng.integers(-4, 4)], np.float32)
+        cases += [(quad, o, z), (side, o, z)]
+    for _ in range(200):
+        p = rng.uniform(0.0, 64.0, 3).astype(np.float32)
+        cases.append((np.stack([p, p, p]), rng.uniform(0.0, 64.0, 3).astype(np.float32), z))
+    return cases
+
+
+def test_ray_triangle_matches_reference():
+    """The mesh queries' ray-triangle test (the CUDA library's mesh.cuh, held bit-exact to the
+    oracle by tests/test_mesh_solids.py) against Obj::RayTriangleTest (src/geom/obj/obj.cpp:354-398)
+    compiled from the reference's sources: the same hits, and the same hit points bit for bit."""
+    from oracle.pyoracle import tri_ray
+    rng = np.random.default_rng(11)
+    cases = _ray_triangle_cases(rng)
+    hits = 0
+    for v, o, d in cases:
+        rh, rp = pyref.ray_triangle(v, o, d)
+        oh, op = tri_ray(v, o, d)
+        assert rh == oh, (v.tolist(), o.tolist(), d.tolist())
+        if rh:
+            hits += 1
+            assert np.array_equal(rp.view(np.uint32), op.view(np.uint32)), (v.tolist(), o.tolist(), d.tolist())
+    assert hits > len(cases) // 4
