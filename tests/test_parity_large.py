@@ -50,17 +50,20 @@ def _max_cell_count(h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [64, 96, 128])
 def test_stage_parity_from_init(n):
-    """C1 / C2 dam break: both sides run their own Init (seeding, density normaliser, first sort
-    and classification), then every stage of the first step is compared."""
+    """The 64^3 and 128^3 dam breaks, and 96^3, whose grid index divisors (n, n + 1, n^2,
+    n (n + 1)) have inexact reciprocals: both sides run their own Init (seeding, density
+    normaliser, first sort and classification), then every stage of the first step is compared."""
     desc = dambreak(n, seed=1)
     prm = params(stop=A.STOP_REL, tol=1e-6)
     ora = RefSim(desc, prm)
     ora.init()
     gpu = Batch([desc], prm)
     gpu.init()
-    assert gpu.count() == ora.count() == {64: 502656, 128: 4021248}[n]
+    assert gpu.count() == ora.count()
+    if n in (64, 128):
+        assert gpu.count() == {64: 502656, 128: 4021248}[n]
     assert gpu.max_density() == ora.max_density()
     assert_bits("init pos", gpu.get_particles()["pos"], ora.get_particles()["pos"])
     assert_bits("init flags", gpu.get_grid(A.GRID_A), ora.get_grid(A.GRID_A))
@@ -72,7 +75,7 @@ def test_stage_parity_from_init(n):
 @pytest.mark.gpu
 @pytest.mark.parametrize("grid_blocks", [0, 24], ids=["resident_grid", "streamed_chunks"])
 def test_stage_parity_64_evolved(grid_blocks):
-    """C1 after ten oracle steps (a sloshing state with crowded cells)."""
+    """The 64^3 dam break after ten oracle steps (a sloshing state with crowded cells)."""
     desc = dambreak(64, seed=1)
     prm = params(stop=A.STOP_REL, tol=1e-6, pcg_grid_blocks=grid_blocks)
     st, P, P64 = _evolve(desc, prm, 10)
@@ -85,7 +88,7 @@ def test_stage_parity_64_evolved(grid_blocks):
 
 @pytest.mark.gpu
 def test_whole_step_from_init_64():
-    """C1: one full step from Init on both sides; flags and SDF are decided before the solve and
+    """The 64^3 dam break: one full step from Init on both sides; flags and SDF are decided before the solve and
     are bit-exact, particle state after the solve agrees to the solve's tolerance."""
     desc = dambreak(64, seed=1)
     prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-6, graph=1)
