@@ -189,16 +189,21 @@ __global__ void k_sort_scatter(DevState S) {
 }
 
 // Restores ascending particle id inside each cell (the reference's append order): cells of up
-// to kSortRegs particles are sorted in registers, larger ones in place.
+// to kSortRegs particles are sorted in registers; larger ones are listed (in the arrival-offset
+// array, free once the scatter has run; `nbig` counts them) for k_sort_big.
 constexpr int kSortRegs = 16;
-__global__ void k_sort_cells(DevState S) {
+__global__ void k_sort_cells(DevState S, uint32_t* nbig) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= S.nc) return;
     uint32_t a = S.start[c], b = S.start[c + 1];
     if (b - a < 2) return;
     uint32_t* seg = S.sid + a;
     uint32_t m = b - a;
-    if (m <= kSortRegs) {
+    if (m > kSortRegs) {
+        S.off[atomicAdd(nbig, 1u)] = (uint32_t)c;  // fewer than np / kSortRegs such cells
+        return;
+    }
+    {
         uint32_t v[kSortRegs];
 #pragma unroll
         for (int i = 0; i < kSortRegs; ++i) v[i] = i < (int)m ? seg[i] : 0xffffffffu;
@@ -214,16 +219,48 @@ __global__ void k_sort_cells(DevState S) {
 #pragma unroll
         for (int i = 0; i < kSortRegs; ++i)
             if (i < (int)m) seg[i] = v[i];
-        return;
     }
-    for (uint32_t i = 1; i < m; ++i) {
-        uint32_t v = seg[i];
-        uint32_t j = i;
-        while (j > 0 && seg[j - 1] > v) {
-            seg[j] = seg[j - 1];
-            --j;
+}
+
+// The listed cells, one warp each: the segment is copied to shared memory and every id is
+// written to its rank, the number of smaller ids in the cell (ids are distinct), so the cell
+// ends in ascending id order as after an insertion sort, in m^2 / 32 comparisons per lane instead
+// of a serial chain of global loads and stores.  A segment beyond the shared copy (more than
+// kBigCell particles in one cell) falls back to one lane's insertion sort in place.
+constexpr int kBigCell = 1024;
+constexpr int kBigWarps = 8;
+constexpr int kSortBigBlocks = 296;  // a grid-stride loop over the listed cells
+__global__ void __launch_bounds__(32 * kBigWarps) k_sort_big(DevState S, const uint32_t* nbig) {
+    __shared__ uint32_t buf[kBigWarps][kBigCell];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t count = *nbig;
+    for (uint32_t q = blockIdx.x * kBigWarps + w; q < count; q += gridDim.x * kBigWarps) {
+        const uint32_t c = S.off[q];
+        const uint32_t a = S.start[c], m = S.start[c + 1] - a;
+        uint32_t* seg = S.sid + a;
+        if (m > (uint32_t)kBigCell) {
+            if (lane == 0)
+                for (uint32_t i = 1; i < m; ++i) {
+                    const uint32_t v = seg[i];
+                    uint32_t j = i;
+                    while (j > 0 && seg[j - 1] > v) {
+                        seg[j] = seg[j - 1];
+                        --j;
+                    }
+                    seg[j] = v;
+                }
+            __syncwarp();
+            continue;
         }
-        seg[j] = v;
+        for (uint32_t i = lane; i < m; i += 32) buf[w][i] = seg[i];
+        __syncwarp();
+        for (uint32_t i = lane; i < m; i += 32) {
+            const uint32_t v = buf[w][i];
+            uint32_t r = 0;
+            for (uint32_t j = 0; j < m; ++j) r += buf[w][j] < v ? 1u : 0u;
+            seg[r] = v;
+        }
+        __syncwarp();
     }
 }
 
@@ -805,10 +842,14 @@ static cudaError_t sort_core(const DevState& S, void* scan_tmp, cudaStream_t st)
     cudaError_t e = launch_scan_u32(S.count, S.start, S.nc, scan_tmp, st);
     if (e != cudaSuccess) return e;
     if (S.np > 0) {
+        // the scan's scratch is free again: its first word counts the cells for k_sort_big
+        uint32_t* nbig = reinterpret_cast<uint32_t*>(scan_tmp);
         k_sort_scatter<<<grid_for(S.np), kBlock, 0, st>>>(S);
-        k_sort_cells<<<grid_for(S.nc), kBlock, 0, st>>>(S);
+        cudaMemsetAsync(nbig, 0, sizeof(uint32_t), st);
+        k_sort_cells<<<grid_for(S.nc), kBlock, 0, st>>>(S, nbig);
+        k_sort_big<<<kSortBigBlocks, 32 * kBigWarps, 0, st>>>(S, nbig);
         k_sort_permute<<<grid_for(S.np), kBlock, 0, st>>>(S);
-        count_launch(3);
+        count_launch(4);
     }
     return cudaGetLastError();
 }
