@@ -883,7 +883,7 @@ ariel_status enqueue_stage(ariel_sim* s, int g, cudaEvent_t* evs = nullptr) {
         case ARIEL_STAGE_SORT: e = launch_sort(S, s->scan_tmp, st); break;
         case ARIEL_STAGE_DENSITY: e = launch_density(S, st); break;
         case ARIEL_STAGE_FORCES: e = launch_forces(S, st); break;
-        case ARIEL_STAGE_P2G: e = launch_p2g(S, st); break;
+        case ARIEL_STAGE_P2G: e = launch_p2g(S, s->prm.p2g_faces, st); break;
         case ARIEL_STAGE_CLASSIFY: e = launch_classify(S, 0, st); break;
         case ARIEL_STAGE_BOUNDARY_DIV: e = launch_boundary_div(S, st); break;
         case ARIEL_STAGE_SOLVE:
@@ -986,6 +986,8 @@ ariel_status check_params(const AsimParams* params) {
     int bx, by, bz;
     sweep_brick(*params, bx, by, bz);
     if (!brick_shape_ok(bx, by, bz)) return ARIEL_ERR_INVALID_ARG;
+    if (params->p2g_faces != 0 && params->p2g_faces != 1 && params->p2g_faces != 2 && params->p2g_faces != 4)
+        return ARIEL_ERR_INVALID_ARG;
     return ARIEL_OK;
 }
 

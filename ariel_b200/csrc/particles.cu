@@ -369,28 +369,43 @@ __global__ void k_forces(DevState S) {
 // SplatParticlesToMACGrid (particlegridoperations.inl:146-249): every face gathers the FLUID
 // particles of its 2x4x4 cell block (GetWallNeighbors, particlegrid.cpp:52-73) with the
 // Sharpen kernel of radius 1.4 cells.  Face-parallel, so no atomics and a fixed order.
+//
+// A thread takes F consecutive faces of one row (same axis, i and j; k, k+1, ...).
+// Their blocks share the x and y cell columns, so the thread walks each column once over the
+// union of the faces' z ranges: every candidate record is loaded once, its x and y distance
+// terms computed once, and the velocity component read once for all the faces it reaches.
+// Each face still sees exactly its own contributors in the reference's order (cells sx, sy, z
+// ascending, ids ascending inside a cell).  For x and y faces a record in the union but outside
+// a face's block (z cells k-2 .. k+1) lies at least 1.5 cells from it along z (gpos is maxd * p
+// clamped, its cell the truncation of gpos clamped to maxd - 1), and one in a cell pruned for
+// that face lies beyond 1.1 radii; both give r2 >= 1.4^2, the test that drops a record, exactly
+// as the per-face walk drops its zero-weight records.  A z face's block spans only cells k-1
+// and k, and records of cell k+1 can lie within the radius, so there each record's cell (from
+// its gpos) selects the two faces whose blocks hold it.
+// Blocks take thirds of the group range in turn (block b: third b % 3), so the three face axes
+// of a region run together and read the particle records from L2 once instead of three times.
 // ------------------------------------------------------------------------------------------
-__global__ void k_p2g(DevState S) {
-    SCENE_PREFIX(S.f_pref);
-    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= S.nf) return;
-    int sc = find_scene(pref_s, S.k, g);
-    const SceneDev& D = S.scenes[sc];
+constexpr long long kP2gThreads = 2500000;
+
+__device__ __forceinline__ float face_offset_z(int axis, int k) { return axis == 2 ? (float)k : k + 0.5f; }
+
+template <int F>
+__device__ __forceinline__ void p2g_row(const DevState& S, const SceneDev& D, int axis, int i, int j, int k, int nk,
+                                        float* __restrict__ out) {
     const int n = D.n;
-    int axis, i, j, k;
-    face_ijk(D, g - D.f_begin, axis, i, j, k);
-    // face centre and GetWallNeighbors block [index - nn, index + nn - 1]
-    float fx, fy, fz;
+    // face centre (x, y shared by the row) and the union of the GetWallNeighbors blocks
+    // [index - nn, index + nn - 1] of faces k .. k + nk - 1
+    float fx, fy;
     int xlo, xhi, ylo, yhi, zlo, zhi;
     if (axis == 0) {
-        fx = (float)i; fy = j + 0.5f; fz = k + 0.5f;
-        xlo = i - 1; xhi = i; ylo = j - 2; yhi = j + 1; zlo = k - 2; zhi = k + 1;
+        fx = (float)i; fy = j + 0.5f;
+        xlo = i - 1; xhi = i; ylo = j - 2; yhi = j + 1; zlo = k - 2; zhi = k + nk;
     } else if (axis == 1) {
-        fx = i + 0.5f; fy = (float)j; fz = k + 0.5f;
-        xlo = i - 2; xhi = i + 1; ylo = j - 1; yhi = j; zlo = k - 2; zhi = k + 1;
+        fx = i + 0.5f; fy = (float)j;
+        xlo = i - 2; xhi = i + 1; ylo = j - 1; yhi = j; zlo = k - 2; zhi = k + nk;
     } else {
-        fx = i + 0.5f; fy = j + 0.5f; fz = (float)k;
-        xlo = i - 2; xhi = i + 1; ylo = j - 2; yhi = j + 1; zlo = k - 1; zhi = k;
+        fx = i + 0.5f; fy = j + 0.5f;
+        xlo = i - 2; xhi = i + 1; ylo = j - 2; yhi = j + 1; zlo = k - 1; zhi = k + nk - 1;
     }
     xlo = max(xlo, 0); xhi = min(xhi, n - 1);
     ylo = max(ylo, 0); yhi = min(yhi, n - 1);
@@ -398,11 +413,19 @@ __global__ void k_p2g(DevState S) {
     const float RE = 1.4f;
     const float RE2 = RE * RE;
     // Cells whose nearest point is farther than the Sharpen radius (with a 10% margin over any
-    // rounding) hold only particles whose weight is exactly 0; skipping them leaves the
-    // contributing particles in the reference's order.
+    // rounding) from every face of the run hold only particles whose weight is exactly 0.  A
+    // cell below the run is nearest to its first face, one above it to its last.
     const float LIM = 1.1f * RE2;
+    const float fz_lo = face_offset_z(axis, k), fz_hi = face_offset_z(axis, k + nk - 1);
+    float fz[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) fz[f] = face_offset_z(axis, k + f);
     const float2 nfxy = make_float2(-fx, -fy);
-    float sumw = 0.0f, sumu = 0.0f;
+    const float* __restrict__ vel = reinterpret_cast<const float*>(S.svel4) + axis;
+    const float maxd_m1 = D.maxd - 1.0f;
+    float sumw[F], sumu[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) sumw[f] = sumu[f] = 0.0f;
     if (zlo <= zhi) {
         for (int sx = xlo; sx <= xhi; ++sx) {
             const float gx = axis_gap2(fx, (float)sx, (float)(sx + 1));
@@ -411,28 +434,76 @@ __global__ void k_p2g(DevState S) {
                 const float gxy = gx + axis_gap2(fy, (float)sy, (float)(sy + 1));
                 if (gxy > LIM) continue;
                 int z0 = zlo, z1 = zhi;
-                while (z0 <= z1 && gxy + axis_gap2(fz, (float)z0, (float)(z0 + 1)) > LIM) ++z0;
-                while (z1 >= z0 && gxy + axis_gap2(fz, (float)z1, (float)(z1 + 1)) > LIM) --z1;
+                while (z0 <= z1 && gxy + axis_gap2(fz_lo, (float)z0, (float)(z0 + 1)) > LIM) ++z0;
+                while (z1 >= z0 && gxy + axis_gap2(fz_hi, (float)z1, (float)(z1 + 1)) > LIM) --z1;
                 if (z0 > z1) continue;
                 long long cb = D.c_begin + ((long long)sx * n + sy) * n;
                 uint32_t a = S.start[cb + z0], b = S.start[cb + z1 + 1];
                 for (uint32_t t = a; t < b; ++t) {
-                    float4 q = S.gpos4[t];
-                    float r2 = sqrlength_xy2(q, nfxy, fz);
-                    // Sharpen is exactly 0 for r2 >= RE^2 (and non-FLUID records are far away)
-                    if (!(r2 < RE2)) continue;
-                    float4 v = S.svel4[t];
-                    float w = q.w * sharpen_k(r2, RE);
-                    float uc = axis == 0 ? v.x : (axis == 1 ? v.y : v.z);
-                    sumu += w * uc;
-                    sumw += w;
+                    const float4 q = S.gpos4[t];
+                    // sqrlength_xy2's sum, (dx^2 + dy^2) + dz^2, with the first term shared
+                    const float2 d = __fadd2_rn(make_float2(q.x, q.y), nfxy);
+                    const float2 s2 = __fmul2_rn(d, d);
+                    const float sxy = s2.x + s2.y;
+                    // faces f_lo .. f_hi of the run have this record's cell in their block
+                    int f_lo = 0, f_hi = nk - 1;
+                    if (axis == 2) {
+                        const int cz = (int)gmin(q.z, maxd_m1);
+                        f_lo = cz - k;
+                        f_hi = min(cz - k + 1, nk - 1);
+                    }
+                    float r2[F];
+                    bool any = false;
+#pragma unroll
+                    for (int f = 0; f < F; ++f) {
+                        const float c = q.z - fz[f];
+                        r2[f] = sxy + c * c;
+                        // Sharpen is exactly 0 for r2 >= RE^2 (and non-FLUID records are far away)
+                        any |= f >= f_lo && f <= f_hi && r2[f] < RE2;
+                    }
+                    if (!any) continue;
+                    const float uc = vel[4 * (size_t)t];
+#pragma unroll
+                    for (int f = 0; f < F; ++f) {
+                        if (f >= f_lo && f <= f_hi && r2[f] < RE2) {
+                            const float w = q.w * sharpen_k(r2[f], RE);
+                            sumu[f] += w * uc;
+                            sumw[f] += w;
+                        }
+                    }
                 }
             }
         }
     }
-    float val = 0.0f;
-    if (sumw > 0) val = sumu / sumw;
-    S.u[g] = val;
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+        if (f < nk) {
+            float val = 0.0f;
+            if (sumw[f] > 0) val = sumu[f] / sumw[f];
+            out[f] = val;
+        }
+    }
+}
+
+// Thread -> group of F faces, with the group range cut in thirds that blocks take in turn;
+// `third` is the number of groups in one third (a multiple of the block size).
+template <int F>
+__global__ void k_p2g(DevState S, long long third) {
+    SCENE_PREFIX(S.f_pref);
+    const long long grp = (long long)(blockIdx.x % 3) * third + (long long)(blockIdx.x / 3) * blockDim.x + threadIdx.x;
+    long long g = grp * F;
+    if (g >= S.nf) return;
+    const long long gend = min(g + F, S.nf);
+    // a group that crosses a row (z faces: rows of n + 1) or a scene is walked in pieces
+    while (g < gend) {
+        const SceneDev& D = S.scenes[find_scene(pref_s, S.k, g)];
+        int axis, i, j, k;
+        face_ijk(D, g - D.f_begin, axis, i, j, k);
+        const int ek = axis == 2 ? D.n + 1 : D.n;
+        const int nk = (int)min((long long)(ek - k), gend - g);
+        p2g_row<F>(S, D, axis, i, j, k, nk, S.u + g);
+        g += nk;
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -887,9 +958,21 @@ cudaError_t launch_forces(const DevState& S, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_p2g(const DevState& S, cudaStream_t st) {
+cudaError_t launch_p2g(const DevState& S, int faces, cudaStream_t st) {
     if (S.nf == 0) return cudaSuccess;
-    k_p2g<<<grid_for(S.nf), kBlock, 0, st>>>(S);
+    // Faces per thread: the largest of 4, 2, 1 that still leaves kP2gThreads threads (longer
+    // runs read fewer records per face but leave too few warps to hide the gathers' latency on
+    // small grids: measured best 1 at 64^3, 2 at 128^3, 4 at 256^3).
+    const int F = faces ? faces : (S.nf >= 4 * kP2gThreads ? 4 : (S.nf >= 2 * kP2gThreads ? 2 : 1));
+    const long long groups = (S.nf + F - 1) / F;
+    const long long third_blocks = (groups + 3LL * kBlock - 1) / (3LL * kBlock);
+    const unsigned blocks = (unsigned)(3 * third_blocks);
+    if (F == 4)
+        k_p2g<4><<<blocks, kBlock, 0, st>>>(S, third_blocks * kBlock);
+    else if (F == 2)
+        k_p2g<2><<<blocks, kBlock, 0, st>>>(S, third_blocks * kBlock);
+    else
+        k_p2g<1><<<blocks, kBlock, 0, st>>>(S, third_blocks * kBlock);
     count_launch();
     return cudaGetLastError();
 }

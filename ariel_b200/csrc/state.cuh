@@ -51,7 +51,8 @@ cudaError_t launch_begin(const DevState& S, cudaStream_t st);
 cudaError_t launch_sort(const DevState& S, void* scan_tmp, cudaStream_t st);
 cudaError_t launch_density(const DevState& S, cudaStream_t st);
 cudaError_t launch_forces(const DevState& S, cudaStream_t st);
-cudaError_t launch_p2g(const DevState& S, cudaStream_t st);
+// faces: faces per thread (1, 2, 4), or 0 to choose by the number of faces
+cudaError_t launch_p2g(const DevState& S, int faces, cudaStream_t st);
 cudaError_t launch_classify(const DevState& S, int init_density, cudaStream_t st);
 cudaError_t launch_boundary_div(const DevState& S, cudaStream_t st);
 cudaError_t launch_gradient(const DevState& S, cudaStream_t st);

@@ -166,6 +166,9 @@ typedef struct AsimParams {
                                    (MIC(0) and the reference's PRef==1 path); results do not depend
                                    on it.  0,0,0 = default 12,12,12.  Limits: i,j <= 31, k <= 63,
                                    product <= 2048, (i+1)(j+1)(k+1) <= 2744 */
+    int32_t p2g_faces;          /* faces of one row each thread of the grid transfer (P2G) takes:
+                                   1, 2 or 4; 0 = chosen by the number of faces.  Results do not
+                                   depend on it */
 } AsimParams;
 
 typedef struct AsimStats {

@@ -134,3 +134,7 @@ def test_argument_limits():
     assert L.ariel_create(C.byref(d), C.byref(p), C.byref(h)) == A.ARIEL_ERR_INVALID_ARG
     arr = (A.AsimSceneDesc * 1025)(*([A.scene_dambreak(8)] * 1025))
     assert L.ariel_create_batch(arr, 1025, C.byref(p), C.byref(h)) == A.ARIEL_ERR_INVALID_ARG
+    d = A.scene_dambreak(16)
+    q = A.params_default()
+    q.p2g_faces = 3
+    assert L.ariel_create(C.byref(d), C.byref(q), C.byref(h)) == A.ARIEL_ERR_INVALID_ARG

@@ -60,6 +60,21 @@ def test_stage_parity(name, desc, steps):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("faces", [1, 2, 4])
+@pytest.mark.parametrize("case", [1, 2, 4, 5], ids=lambda i: CASES[i][0])
+def test_p2g_faces_per_thread(case, faces):
+    """The grid transfer gives the same bits whichever number of consecutive faces of a row
+    each thread gathers (runs cross rows of n + 1 z faces, and the odd grid of 13 cells has no
+    row length divisible by 2 or 4)."""
+    name, desc, steps = CASES[case]
+    prm = params(stop=A.STOP_REL, tol=1e-6, p2g_faces=faces)
+    ora, gpu = _pair(desc, steps, prm)
+    stage_parity("%s_f%d" % (name, faces), gpu, ora)
+    ora.close()
+    gpu.close()
+
+
+@pytest.mark.gpu
 def test_gpu_matches_numpy_golden():
     """The CUDA stages against the independent numpy restatement's committed outputs."""
     import os

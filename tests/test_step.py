@@ -58,12 +58,14 @@ def test_multistep_properties():
 
 
 @pytest.mark.gpu
-def test_batch_equals_alone():
+@pytest.mark.parametrize("p2g_faces", [0, 2, 4])
+def test_batch_equals_alone(p2g_faces):
     """Scenes of different sizes stepped in one batch give bit-identical results to each scene
-    stepped alone (chunked reductions depend only on each scene's own cells)."""
+    stepped alone (chunked reductions depend only on each scene's own cells), also when the
+    batch's grid transfer runs several faces per thread across row and scene boundaries."""
     descs = [dambreak(16, seed=1), dambreak(24, seed=2, hi=(0.3, 0.5, 1.0)), dambreak(12, seed=3)]
     prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1)
-    batch = Batch(descs, prm)
+    batch = Batch(descs, params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, p2g_faces=p2g_faces))
     batch.init()
     batch.step(4)
     for i, d in enumerate(descs):
