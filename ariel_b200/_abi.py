@@ -72,7 +72,8 @@ class AsimParams(C.Structure):
         ("rng_seed", C.c_uint64), ("use_graph", C.c_int32), ("timing", C.c_int32),
         ("barrier_timeout_ms", C.c_double), ("fail_on_not_converged", C.c_int32),
         ("pcg_blocks_per_sm", C.c_int32), ("pcg_grid_blocks", C.c_int32), ("sweep_brick", C.c_int32 * 3),
-        ("p2g_faces", C.c_int32),
+        ("p2g_faces", C.c_int32), ("reseed_every", C.c_int32), ("reseed_min", C.c_int32),
+        ("reseed_max", C.c_int32),
     ]
 
 

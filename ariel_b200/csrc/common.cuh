@@ -46,6 +46,8 @@ struct SceneDev {
     long long f_begin;
     unsigned long long rng_seed;
     int resample_every;  // resample on frames divisible by this (1: every step, flip.cpp:121)
+    int reseed_every;    // reseed on frames divisible by this (0: never)
+    int reseed_min, reseed_max;  // particle-count bounds of the reseeding pass
     // When a kernel radius squared (in float) is a power of two, r2 / (h*h) equals
     // r2 * (1 / (h*h)) exactly, so the division can be replaced by a multiplication.
     int dens_pow2;       // dens_h * dens_h is a power of two
@@ -141,6 +143,7 @@ __host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, ui
 }
 constexpr uint32_t kTagSeed = 0x53454544u;      // "SEED"
 constexpr uint32_t kTagResample = 0x5245534Du;  // "RESM"
+constexpr uint32_t kTagReseed = 0x52534544u;    // "RSED"
 
 // ------------------------------------------------------------------------------------------
 // Grid index decoding without integer division (a 64-bit division is a long instruction

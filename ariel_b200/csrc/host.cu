@@ -160,6 +160,7 @@ void free_all(ariel_sim* s) { free_bufs(s, false); }
 struct Layout {
     long long k = 0, np = 0, nc = 0, nf = 0, ns = 0, maxch = 0, nbricks = 0, mesh_nodes = 0, mesh_tris = 0;
     bool any_solid = false;
+    bool any_reseed = false;
     int mode = kRef32;
 };
 
@@ -174,6 +175,12 @@ void sweep_brick(const AsimParams& p, int& bx, int& by, int& bz) {
         by = 12;
         bz = 12;
     }
+}
+
+// Particle-count bounds of the reseeding pass (0 selects the defaults 6 and 10).
+void reseed_bounds(const AsimParams& p, int& lo, int& hi) {
+    lo = p.reseed_min > 0 ? p.reseed_min : 6;
+    hi = p.reseed_max > 0 ? p.reseed_max : 10;
 }
 
 long long bricks_of(int n, int bx, int by, int bz) {
@@ -222,6 +229,12 @@ long long layout_bytes(const Layout& L) {
     add(nf, 4);      // pu
     add(1, 4);       // dev_error
     add((long long)scan_tmp_bytes(nc), 1);
+    if (L.any_reseed) {
+        add(nc, 4);      // reseed: excess
+        add(nc + 1, 4);  // its scan
+        add(nc, 4);      // deficit
+        add(nc + 1, 4);  // its scan
+    }
     add(nc, 4);      // FLUID list
     add(nc, 16);     // FLUID-list records
     add(k + 1, 8);
@@ -429,6 +442,8 @@ SceneDev make_scene(const AsimSceneDesc& d, const AsimParams& p) {
                                   d.solid[i].center[2] * D.maxd, d.solid[i].radius * D.maxd);
     D.rng_seed = p.rng_seed;
     D.resample_every = p.resample_every;
+    D.reseed_every = p.reseed_every;
+    reseed_bounds(p, D.reseed_min, D.reseed_max);
     auto pow2 = [](float v, float* inv) {
         int e = 0;
         float m = std::frexp(v, &e);
@@ -461,6 +476,7 @@ long long state_bytes(const std::vector<AsimSceneDesc>& descs, const std::vector
     Layout L;
     L.k = (long long)descs.size();
     L.mode = mode_of(prm);
+    L.any_reseed = prm.reseed_every > 0;
     int bx, by, bz;
     sweep_brick(prm, bx, by, bz);
     for (size_t i = 0; i < descs.size(); ++i) {
@@ -572,6 +588,13 @@ ariel_status build_state(ariel_sim* s, std::vector<HostParticles>& hp, const ari
     char* tmp = nullptr;
     ARIEL_TRY(dalloc(s, &tmp, st_bytes));
     s->scan_tmp = tmp;
+    S.any_reseed = s->prm.reseed_every > 0;
+    if (S.any_reseed) {
+        ARIEL_TRY(dalloc(s, &S.rs_excess, nc));
+        ARIEL_TRY(dalloc(s, &S.rs_escan, nc + 1));
+        ARIEL_TRY(dalloc(s, &S.rs_deficit, nc));
+        ARIEL_TRY(dalloc(s, &S.rs_dscan, nc + 1));
+    }
     // pressure solve
     PcgArgs& A = s->PA;
     A = PcgArgs{};
@@ -987,6 +1010,11 @@ ariel_status check_params(const AsimParams* params) {
     sweep_brick(*params, bx, by, bz);
     if (!brick_shape_ok(bx, by, bz)) return ARIEL_ERR_INVALID_ARG;
     if (params->p2g_faces != 0 && params->p2g_faces != 1 && params->p2g_faces != 2 && params->p2g_faces != 4)
+        return ARIEL_ERR_INVALID_ARG;
+    int rmin, rmax;
+    reseed_bounds(*params, rmin, rmax);
+    if (params->reseed_every < 0 || params->reseed_min < 0 || params->reseed_max < 0 || rmin > rmax ||
+        rmax > 65535)
         return ARIEL_ERR_INVALID_ARG;
     return ARIEL_OK;
 }

@@ -843,6 +843,93 @@ __global__ void __launch_bounds__(kBlock, 4) k_resample_velocity(DevState S) {
     S.vel4[g] = make_float4(u.x, u.y, u.z, v4.w);
 }
 
+// ------------------------------------------------------------------------------------------
+// Reseeding (no counterpart in the reference, which never adds or removes particles).  On
+// frames divisible by reseed_every, after the resampler, particles move from crowded cells to
+// sparse interior ones; the particle count, ids, masses and types are kept.  The cells are
+// counted by the resampler's own Sort (the positions after advection; the resampler's moves are
+// a fraction of a cell).  A FLUID cell holding m > reseed_max particles gives m - reseed_max of
+// them, its highest ids first; an interior FLUID cell (all six neighbours FLUID) holding
+// m < reseed_min receives reseed_min - m.  Within each scene the r-th given particle (cells in
+// index order) fills the r-th received place (cells in index order) while both last.  A moved
+// particle lands at a Philox-drawn point of its new cell, at least 5% of a cell from its faces,
+// and takes the grid's PIC velocity there.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool reseed_frame(const SceneDev& D) {
+    return D.reseed_every > 0 && D.frame % D.reseed_every == 0;
+}
+
+__global__ void k_reseed_count(DevState S) {
+    SCENE_PREFIX(S.c_pref);
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= S.nc) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, c)];
+    uint32_t give = 0, take = 0;
+    if (reseed_frame(D) && S.flags[c] == ARIEL_FLUID) {
+        const uint32_t m = S.count[c];
+        if (m > (uint32_t)D.reseed_max) {
+            give = m - (uint32_t)D.reseed_max;
+        } else if (m < (uint32_t)D.reseed_min) {
+            const int n = D.n;
+            int i, j, k;
+            cell_ijk(D, c - D.c_begin, i, j, k);
+            bool interior = i > 0 && i < n - 1 && j > 0 && j < n - 1 && k > 0 && k < n - 1;
+            if (interior) {
+                const long long nn = (long long)n * n;
+                interior = S.flags[c - nn] == ARIEL_FLUID && S.flags[c + nn] == ARIEL_FLUID &&
+                           S.flags[c - n] == ARIEL_FLUID && S.flags[c + n] == ARIEL_FLUID &&
+                           S.flags[c - 1] == ARIEL_FLUID && S.flags[c + 1] == ARIEL_FLUID;
+            }
+            if (interior) take = (uint32_t)D.reseed_min - m;
+        }
+    }
+    S.rs_excess[c] = give;
+    S.rs_deficit[c] = take;
+}
+
+__global__ void k_reseed_move(DevState S) {
+    SCENE_PREFIX(S.c_pref);
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= S.nc) return;
+    const uint32_t give = S.rs_excess[c];
+    if (give == 0) return;
+    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, c)];
+    const int n = D.n;
+    const long long cb = D.c_begin, ce = cb + (long long)n * n * n;
+    const uint32_t d0 = S.rs_dscan[cb], dtot = S.rs_dscan[ce] - d0;
+    const uint32_t r0 = S.rs_escan[c] - S.rs_escan[cb];
+    const uint32_t last = S.start[c + 1] - 1;  // slot of the cell's highest id
+    const float maxd = D.maxd;
+    for (uint32_t u = 0; u < give && r0 + u < dtot; ++u) {
+        const uint32_t g = S.sid[last - u];
+        if (type_of(S.vel4[g]) != ARIEL_FLUID) continue;
+        // the receiving cell q: rs_dscan[q] <= d0 + r < rs_dscan[q + 1] (the largest q with
+        // rs_dscan[q] <= d0 + r; the scan does not decrease)
+        const uint32_t want = d0 + r0 + u;
+        long long lo = cb, hi = ce - 1;
+        while (lo < hi) {
+            const long long mid = (lo + hi + 1) >> 1;
+            if (S.rs_dscan[mid] <= want)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        int i, j, k;
+        cell_ijk(D, lo - cb, i, j, k);
+        const uint4 rv = philox4x32_10(make_uint4(g - (uint32_t)D.p_begin, (uint32_t)D.frame, 0u, kTagReseed),
+                                       (uint32_t)D.rng_seed, (uint32_t)(D.rng_seed >> 32));
+        const float k24 = 1.0f / 16777216.0f;
+        const float fx = 0.05f + 0.9f * ((float)(rv.x >> 8) * k24);
+        const float fy = 0.05f + 0.9f * ((float)(rv.y >> 8) * k24);
+        const float fz = 0.05f + 0.9f * ((float)(rv.z >> 8) * k24);
+        const float3 p = make_float3(((float)i + fx) / maxd, ((float)j + fy) / maxd, ((float)k + fz) / maxd);
+        const float3 v = interp_vel(S.u + D.f_begin, n, p);
+        const float4 p4 = S.pos4[g], v4 = S.vel4[g];
+        S.pos4[g] = make_float4(p.x, p.y, p.z, p4.w);
+        S.vel4[g] = make_float4(v.x, v.y, v.z, v4.w);
+    }
+}
+
 __global__ void k_unpack_state(float4* pos4, float4* vel4, const float* __restrict__ pos,
                                const float* __restrict__ vel, long long n, int* err) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -993,6 +1080,17 @@ cudaError_t launch_resample(const DevState& S, void* scan_tmp, cudaStream_t st) 
     k_resample_spring<<<grid_for(S.np), kBlock, 0, st>>>(S);
     k_resample_velocity<<<grid_for(S.np), kBlock, 0, st>>>(S);
     count_launch(2);
+    if (S.any_reseed) {
+        // the kernels return at once on frames without reseeding; the scans stay (cheap)
+        k_reseed_count<<<grid_for(S.nc), kBlock, 0, st>>>(S);
+        count_launch();
+        e = launch_scan_u32(S.rs_excess, S.rs_escan, S.nc, scan_tmp, st);
+        if (e != cudaSuccess) return e;
+        e = launch_scan_u32(S.rs_deficit, S.rs_dscan, S.nc, scan_tmp, st);
+        if (e != cudaSuccess) return e;
+        k_reseed_move<<<grid_for(S.nc), kBlock, 0, st>>>(S);
+        count_launch();
+    }
     return cudaGetLastError();
 }
 

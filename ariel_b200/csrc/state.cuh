@@ -44,6 +44,13 @@ struct DevState {
     float* pu;  // m_mgrid_previous faces
     // error word for bounded device waits
     int* dev_error;
+    // reseeding pass (allocated when it is enabled): per cell the particles to give and to
+    // receive, and their exclusive scans (nc + 1 entries)
+    int any_reseed;
+    uint32_t* rs_excess;
+    uint32_t* rs_escan;
+    uint32_t* rs_deficit;
+    uint32_t* rs_dscan;
 };
 
 // Launchers (each returns cudaGetLastError()).

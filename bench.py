@@ -151,7 +151,7 @@ PRECOND = "ref"
 INNER_TOL = 0.0
 
 
-def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
+def make_params(A, precision, tol, timing=1, graph=1, resample_every=1, reseed_every=0):
     p = A.params_default()
     p.precision = precision
     p.precond = A.PRECOND_MIC0 if PRECOND == "mic0" else A.PRECOND_REF
@@ -160,6 +160,7 @@ def make_params(A, precision, tol, timing=1, graph=1, resample_every=1):
     p.use_graph = graph
     p.timing = timing
     p.resample_every = resample_every
+    p.reseed_every = reseed_every  # bounds: the library's defaults, 6 and 10 particles per cell
     if INNER_TOL > 0:
         p.inner_tol = INNER_TOL
     return p
@@ -401,7 +402,8 @@ def config_dict(args, n_particles, ws):
                 "l2": "inputs larger than L2 (particle state %.0f MB)" % (n_particles * 64 / 1e6)}
     if args.workload == "sphere":
         return {"workload": "dam break %d^3 with a static solid sphere (c=(.6,.3,.5), r=.15), %d particles, "
-                            "dt 1/480, resampling every 5 steps, %s PCG to %g relative residual"
+                            "dt 1/480, resampling and reseeding to 6-10 particles per cell every 5 steps, "
+                            "%s PCG to %g relative residual"
                             % (args.n, n_particles, args.precision, args.tol),
                 "grid": args.n, "particles_per_scene": n_particles, "precision": args.precision,
                 "tolerance": args.tol, "parallelism": "replicas" if ws > 1 else "single",
@@ -550,6 +552,7 @@ def main():
     prec = {"mixed": A.PREC_MIXED, "fp64": A.PREC_FP64, "ref32": A.PREC_REF32}[args.precision]
     from ariel_b200 import workloads as W
     resample_every = 1
+    reseed_every = 0
     if args.workload == "serve":
         rc = serve_arm(args, A, prec, ws, rank, pg, gpu_index)
         if pg:
@@ -561,11 +564,12 @@ def main():
     elif args.workload == "sphere":
         desc = W.sphere_dambreak(args.n, seed=replica_seed(rank))
         resample_every = 5
+        reseed_every = 5
     else:
         desc = A.scene_dambreak(args.n, seed=replica_seed(rank))
     barrier = (lambda: pg.barrier()) if pg else None
     sampler = ClockSampler(gpu_index)
-    prm = make_params(A, prec, args.tol, resample_every=resample_every)
+    prm = make_params(A, prec, args.tol, resample_every=resample_every, reseed_every=reseed_every)
     tune_report = None
     if args.autotune:
         from ariel_b200 import autotune
@@ -664,7 +668,8 @@ def main():
     b.close()
 
     if not args.no_fp64_compare and args.precision != "fp64":
-        b64, r64 = run_gpu_pass(A, Batch, desc, make_params(A, A.PREC_FP64, args.tol, resample_every=resample_every),
+        b64, r64 = run_gpu_pass(A, Batch, desc, make_params(A, A.PREC_FP64, args.tol, resample_every=resample_every,
+                                                                reseed_every=reseed_every),
                                 args.steps, args.warmup)
         b64.close()
         t64 = r64["totals"]

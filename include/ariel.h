@@ -169,6 +169,13 @@ typedef struct AsimParams {
     int32_t p2g_faces;          /* faces of one row each thread of the grid transfer (P2G) takes:
                                    1, 2 or 4; 0 = chosen by the number of faces.  Results do not
                                    depend on it */
+    int32_t reseed_every;       /* 0 = off; else, on frames divisible by it and after resampling,
+                                   particles above reseed_max in a FLUID cell move to interior FLUID
+                                   cells (all six neighbours FLUID) below reseed_min.  The particle
+                                   count is kept.  No counterpart in the reference, which never
+                                   adds or removes particles */
+    int32_t reseed_min;         /* 0 -> 6 */
+    int32_t reseed_max;         /* 0 -> 10 */
 } AsimParams;
 
 typedef struct AsimStats {
