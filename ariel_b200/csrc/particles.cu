@@ -887,37 +887,45 @@ __global__ void k_reseed_count(DevState S) {
     S.rs_deficit[c] = take;
 }
 
+// One thread per given particle (grid-stride over the scan's total, so a crowded cell's
+// particles spread over many threads): the giving cell and the receiving cell are found by
+// binary search over the two scans.
+__device__ __forceinline__ long long last_at_or_below(const uint32_t* __restrict__ scan, long long lo, long long hi,
+                                                      uint32_t v) {
+    // the largest q in [lo, hi] with scan[q] <= v (scan does not decrease; scan[lo] <= v)
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (scan[mid] <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+constexpr int kReseedBlocks = 4 * 148;  // four blocks on each of a B200's SMs
+
 __global__ void k_reseed_move(DevState S) {
     SCENE_PREFIX(S.c_pref);
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= S.nc) return;
-    const uint32_t give = S.rs_excess[c];
-    if (give == 0) return;
-    const SceneDev& D = S.scenes[find_scene(pref_s, S.k, c)];
-    const int n = D.n;
-    const long long cb = D.c_begin, ce = cb + (long long)n * n * n;
-    const uint32_t d0 = S.rs_dscan[cb], dtot = S.rs_dscan[ce] - d0;
-    const uint32_t r0 = S.rs_escan[c] - S.rs_escan[cb];
-    const uint32_t last = S.start[c + 1] - 1;  // slot of the cell's highest id
-    const float maxd = D.maxd;
-    for (uint32_t u = 0; u < give && r0 + u < dtot; ++u) {
-        const uint32_t g = S.sid[last - u];
+    const uint32_t total = S.rs_escan[S.nc];
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < total; x += gridDim.x * blockDim.x) {
+        // the giving cell c (rs_escan[c] <= x < rs_escan[c + 1]) and the unit u inside it
+        const long long c = last_at_or_below(S.rs_escan, 0, S.nc - 1, x);
+        const uint32_t u = x - S.rs_escan[c];
+        const SceneDev& D = S.scenes[find_scene(pref_s, S.k, c)];
+        const int n = D.n;
+        const long long cb = D.c_begin, ce = cb + (long long)n * n * n;
+        const uint32_t d0 = S.rs_dscan[cb], dtot = S.rs_dscan[ce] - d0;
+        const uint32_t r = x - S.rs_escan[cb];  // rank of this unit in its scene
+        if (r >= dtot) continue;
+        const uint32_t g = S.sid[S.start[c + 1] - 1 - u];  // the cell's highest ids first
         if (type_of(S.vel4[g]) != ARIEL_FLUID) continue;
-        // the receiving cell q: rs_dscan[q] <= d0 + r < rs_dscan[q + 1] (the largest q with
-        // rs_dscan[q] <= d0 + r; the scan does not decrease)
-        const uint32_t want = d0 + r0 + u;
-        long long lo = cb, hi = ce - 1;
-        while (lo < hi) {
-            const long long mid = (lo + hi + 1) >> 1;
-            if (S.rs_dscan[mid] <= want)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
+        const long long q = last_at_or_below(S.rs_dscan, cb, ce - 1, d0 + r);
         int i, j, k;
-        cell_ijk(D, lo - cb, i, j, k);
+        cell_ijk(D, q - cb, i, j, k);
         const uint4 rv = philox4x32_10(make_uint4(g - (uint32_t)D.p_begin, (uint32_t)D.frame, 0u, kTagReseed),
                                        (uint32_t)D.rng_seed, (uint32_t)(D.rng_seed >> 32));
+        const float maxd = D.maxd;
         const float k24 = 1.0f / 16777216.0f;
         const float fx = 0.05f + 0.9f * ((float)(rv.x >> 8) * k24);
         const float fy = 0.05f + 0.9f * ((float)(rv.y >> 8) * k24);
@@ -1088,7 +1096,7 @@ cudaError_t launch_resample(const DevState& S, void* scan_tmp, cudaStream_t st) 
         if (e != cudaSuccess) return e;
         e = launch_scan_u32(S.rs_deficit, S.rs_dscan, S.nc, scan_tmp, st);
         if (e != cudaSuccess) return e;
-        k_reseed_move<<<grid_for(S.nc), kBlock, 0, st>>>(S);
+        k_reseed_move<<<kReseedBlocks, kBlock, 0, st>>>(S);
         count_launch();
     }
     return cudaGetLastError();

@@ -40,9 +40,10 @@ def _rule(cell, flags, n, lo, hi):
     return np.array(movers[:m], np.int64), places[:m], counts
 
 
-def _crowded_state(n):
-    """A 16^3 dam break's initial particles, with three interior cells crowded by particles
-    taken from nine others (which drop below six)."""
+def _crowded_state(n, big):
+    """A 16^3 dam break's initial particles (8 in every cell of the block) and its FLUID flags.
+    Either three interior cells are crowded by 4 particles from each of nine others, or one
+    interior cell takes every particle of 40 others (328 particles in one cell)."""
     desc = dambreak(n, seed=3)
     b = Batch([desc], params())
     b.init()
@@ -50,28 +51,36 @@ def _crowded_state(n):
     b.close()
     pos = st["pos"].copy()
     cell = _cells(pos, n)
+    flags = np.where(np.bincount(cell, minlength=n ** 3) > 0, A.FLUID, A.AIR).astype(np.uint8).reshape(n, n, n)
     rng = np.random.default_rng(5)
-    sinks = [(2, 3, 5), (3, 4, 9), (4, 2, 12)]
-    sources = [(2, 5, 3), (3, 2, 4), (4, 4, 6), (2, 6, 8), (3, 3, 11), (4, 5, 13), (2, 2, 10), (3, 6, 7),
-               (4, 3, 2)]
+    if big:
+        sinks = [(3, 4, 8)]
+        sources = [(i, j, k) for i in (1, 2, 4, 5) for j in (2, 6) for k in (2, 4, 7, 10, 13)]
+        take = 8
+    else:
+        sinks = [(2, 3, 5), (3, 4, 9), (4, 2, 12)]
+        sources = [(2, 5, 3), (3, 2, 4), (4, 4, 6), (2, 6, 8), (3, 3, 11), (4, 5, 13), (2, 2, 10), (3, 6, 7),
+                   (4, 3, 2)]
+        take = 4
     for si, s in enumerate(sources):
-        ids = np.nonzero(cell == (s[0] * n + s[1]) * n + s[2])[0][:4]
-        t = sinks[si % 3]
+        ids = np.nonzero(cell == (s[0] * n + s[1]) * n + s[2])[0][:take]
+        t = sinks[si % len(sinks)]
         pos[ids] = (np.array(t, np.float32) + rng.uniform(0.1, 0.9, (len(ids), 3)).astype(np.float32)) / n
-    return desc, st, pos
+    return desc, st, pos, flags
 
 
 @pytest.mark.gpu
-def test_reseed_follows_the_rule():
+@pytest.mark.parametrize("big", [False, True], ids=["three_cells", "one_cell_of_328"])
+def test_reseed_follows_the_rule(big):
     n, lo, hi = 16, 6, 10
-    desc, st, pos = _crowded_state(n)
+    desc, st, pos, flags = _crowded_state(n, big)
     cell = _cells(pos, n)
     counts = np.bincount(cell, minlength=n ** 3)
-    flags = np.where(counts > 0, A.FLUID, A.AIR).astype(np.uint8).reshape(n, n, n)
     movers, places, _ = _rule(cell, flags, n, lo, hi)
-    # the sinks hold 20 (10 to give), the sources 4 (2 to receive): 18 move, and the last sink
-    # in index order keeps its crowd
-    assert len(movers) == 18
+    # three cells: the sinks hold 20 (10 to give), the sources 4 (2 to receive), so 18 move and
+    # the last sink in index order keeps its crowd.  One cell: it holds 328 (318 to give), the
+    # 40 emptied cells receive 6 each
+    assert len(movers) == (240 if big else 18)
     prm = params(resample_every=0, reseed_every=1, reseed_min=lo, reseed_max=hi)
     g = Batch([desc], prm)
     g.set_particles(pos, st["vel"], st["mass"], st["type"])
