@@ -110,7 +110,8 @@ def test_whole_step_from_init_64():
 
 @pytest.mark.gpu
 def test_stage_parity_sphere_resample_64():
-    """Config 3's shape at 64^3: evolved by the oracle to frame 4 with resampling every 5th step,
+    """The sphere scene (dam break with a solid sphere at (.6, .3, .5), r .15, dt 1/480) at 64^3:
+    evolved by the oracle to frame 4 with resampling every 5th step,
     then one step with resampling on, stage by stage (sphere push-out, solid constraints and the
     resampler's springs and jitter included)."""
     desc = dambreak(64, seed=3, hi=(0.35, 0.5, 1.0), spheres=[((0.6, 0.3, 0.5), 0.15)])

@@ -49,7 +49,7 @@ WHOLE = [
     ("density025_n10", scene(10, 17, density=0.25), 2),
     ("two_spheres18", scene(18, 19, hi=(0.5, 0.7, 1.0), spheres=[((0.7, 0.25, 0.3), 0.12), ((0.7, 0.25, 0.7), 0.12)]), 4),
     # the 64^3 dam break (502,656 particles), two steps from Init
-    ("dambreak64_C1", scene(64, 1), 2),
+    ("dambreak64", scene(64, 1), 2),
 ]
 
 
