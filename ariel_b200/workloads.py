@@ -3,8 +3,8 @@
 - ``dambreak(n)``: liquid block x in [0,.4], y in [0,.6], z in [0,1], 8 particles per cell
   (lattice density 0.5) jittered inside their sub-cells, gravity -9.8 y, dt 1/240.
 - ``sphere_dambreak(n)``: liquid block x in [0,.35], y in [0,.5], z in [0,1] with a static
-  solid sphere of centre (.6,.3,.5) and radius .15, dt 1/480; stepped with resampling every
-  5th step.
+  solid sphere of centre (.6,.3,.5) and radius .15, dt 1/480; the benchmark steps it with
+  resampling and reseeding (6-10 particles per cell) every 5th step.
 - ``uneven_batch(k, seed)``: k scenes with grid sizes drawn from {32,48,64,96,128} and one
   liquid block each filling 20-50% of its domain.
 - ``arrival_stream(rate, duration, seed)``: Poisson arrivals (exponential gaps of mean
