@@ -131,7 +131,8 @@ def test_reseed_batch_equals_alone():
     """A batch of scenes (one with a solid sphere), resampled and reseeded every second step,
     gives each scene exactly what it gives stepped alone."""
     descs = [dambreak(24, seed=2, hi=(0.35, 0.5, 1.0), spheres=[((0.6, 0.3, 0.5), 0.15)]), dambreak(16, seed=4)]
-    prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, resample_every=2, reseed_every=2)
+    prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, resample_every=2, reseed_every=2,
+                 reseed_min=8, reseed_max=8)
     batch = Batch(descs, prm)
     batch.init()
     batch.step(6)
@@ -162,3 +163,24 @@ def test_reseed_arguments():
         for k, v in kw.items():
             setattr(p, k, v)
         assert L.ariel_create(C.byref(d), C.byref(p), C.byref(h)) == A.ARIEL_ERR_INVALID_ARG, kw
+
+
+@pytest.mark.gpu
+def test_reseed_moves_particles_in_a_running_scene():
+    """In an evolving dam break with bounds of 8 and 8, reseeding frames move particles (the
+    positions differ from the same run without reseeding) while the count and the particles'
+    masses and types stay."""
+    d = dambreak(16, seed=4)
+    runs = []
+    for every in (0, 2):
+        b = Batch([d], params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, reseed_every=every,
+                              reseed_min=8, reseed_max=8))
+        b.init()
+        b.step(6)
+        runs.append(b.get_particles())
+        b.close()
+    assert len(runs[0]["pos"]) == len(runs[1]["pos"])
+    assert not np.array_equal(runs[0]["pos"], runs[1]["pos"])
+    assert_bits("mass", runs[1]["mass"], runs[0]["mass"])
+    assert_bits("type", runs[1]["type"], runs[0]["type"])
+    assert np.isfinite(runs[1]["pos"]).all() and np.isfinite(runs[1]["vel"]).all()

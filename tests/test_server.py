@@ -43,8 +43,12 @@ def _scenes():
 
 
 @pytest.mark.gpu
-def test_served_equals_alone():
-    prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1)
+@pytest.mark.parametrize("reseed_every", [0, 2])
+def test_served_equals_alone(reseed_every):
+    # with reseeding (bounds of 8 and 8, so that the evolving dam breaks do move particles),
+    # each scene reseeds on its own frames whatever batch it runs in
+    prm = params(precision=A.PREC_MIXED, stop=A.STOP_REL, tol=1e-5, graph=1, reseed_every=reseed_every,
+                 reseed_min=8, reseed_max=8)
     scenes = _scenes()
     with Server(prm, max_live=8) as srv:
         ids = [srv.submit(*scenes[0])]
