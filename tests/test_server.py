@@ -142,3 +142,8 @@ def test_server_without_device_and_footprint_on_host():
     assert state_bytes([dambreak(32)], fp64) > b32
     both = state_bytes([dambreak(16), dambreak(32)], mixed)
     assert abs(both - (b16 + b32)) <= 64 * 256  # per-handle buffers counted once
+    # reseeding adds its per-cell counts and their scans, each rounded to 256 bytes
+    nc = 16 ** 3
+    r256 = lambda b: (b + 255) // 256 * 256
+    reseed = state_bytes([dambreak(16)], params(precision=A.PREC_MIXED, reseed_every=2))
+    assert reseed - b16 == 2 * r256(4 * nc) + 2 * r256(4 * (nc + 1))
