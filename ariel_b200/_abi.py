@@ -63,6 +63,13 @@ class AsimSceneDesc(C.Structure):
     ]
 
 
+class AsimSceneInfo(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int32), ("reserved", C.c_int32), ("density", C.c_double), ("step_size", C.c_double),
+        ("partio_output", C.c_char * 512), ("vdb_output", C.c_char * 512), ("mesh_output", C.c_char * 512),
+    ]
+
+
 class AsimParams(C.Structure):
     _fields_ = [
         ("picflip", C.c_float), ("subcell", C.c_int32), ("precond", C.c_int32),

@@ -20,6 +20,11 @@ SIGNATURES = {
     "ariel_scene_dambreak": ([C.POINTER(A.AsimSceneDesc), C.c_int32], None),
     "ariel_mesh_create": ([_vp, C.c_int32, _vp, C.c_int32, _vp, C.c_float, C.POINTER(C.c_int32)], C.c_int),
     "ariel_mesh_destroy": ([C.c_int32], C.c_int),
+    "ariel_mesh_info": ([C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp, C.POINTER(C.c_float)], C.c_int),
+    "ariel_scene_load": ([C.c_char_p, C.c_float, C.c_uint64, C.POINTER(A.AsimSceneDesc), C.POINTER(A.AsimSceneInfo),
+                          C.c_char_p, C.c_int32], C.c_int),
+    "ariel_scene_parse": ([C.c_char_p, C.c_char_p, C.c_float, C.c_uint64, C.POINTER(A.AsimSceneDesc),
+                           C.POINTER(A.AsimSceneInfo), C.c_char_p, C.c_int32], C.c_int),
     "ariel_get_level_set": ([_vp, C.c_int32, _vp, C.c_int64], C.c_int),
     "ariel_surface_mesh": ([_vp, C.c_int32, _vp, C.c_int64, _vp, C.c_int64, C.POINTER(C.c_int64),
                             C.POINTER(C.c_int64)], C.c_int),

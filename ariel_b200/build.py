@@ -14,7 +14,7 @@ SRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(HERE, "_build")
 SO = os.path.join(OUT_DIR, "libariel_b200.so")
-SOURCES = ["scan.cu", "particles.cu", "grid.cu", "pcg.cu", "host.cu", "server.cu", "noalloc.cu", "mesh.cu", "surface.cu"]
+SOURCES = ["scan.cu", "particles.cu", "grid.cu", "pcg.cu", "host.cu", "server.cu", "noalloc.cu", "mesh.cu", "surface.cu", "sceneload.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

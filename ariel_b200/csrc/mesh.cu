@@ -211,4 +211,18 @@ ariel_status ariel_mesh_destroy(int32_t mesh_id) {
     return g_meshes.erase(mesh_id) ? ARIEL_OK : ARIEL_ERR_INVALID_ARG;
 }
 
+ariel_status ariel_mesh_info(int32_t mesh_id, int32_t* n_vertices, int32_t* n_triangles, float* translate,
+                             float* scale) {
+    std::lock_guard<std::mutex> lock(g_mesh_mutex);
+    auto it = g_meshes.find(mesh_id);
+    if (it == g_meshes.end()) return ARIEL_ERR_INVALID_ARG;
+    const MeshObj& m = *it->second;
+    if (n_vertices) *n_vertices = (int32_t)(m.vertices.size() / 3);
+    if (n_triangles) *n_triangles = (int32_t)(m.triangles.size() / 3);
+    if (translate)
+        for (int a = 0; a < 3; ++a) translate[a] = m.translate[a];
+    if (scale) *scale = m.scale;
+    return ARIEL_OK;
+}
+
 }  // extern "C"

@@ -356,6 +356,21 @@ class Mesh:
         self.id = mid.value
         self.vertices, self.triangles, self.translate, self.scale = v, t, tr, float(scale)
 
+    @classmethod
+    def adopt(cls, mesh_id):
+        """Takes ownership of a mesh the library registered itself (ariel_scene_load): its id,
+        placement and counts; it is destroyed with this object."""
+        m = cls.__new__(cls)
+        m.L = lib()
+        nv, nt, sc = C.c_int32(), C.c_int32(), C.c_float()
+        tr = np.zeros(3, np.float32)
+        check(m.L.ariel_mesh_info(mesh_id, C.byref(nv), C.byref(nt), _p(tr), C.byref(sc)), "ariel_mesh_info")
+        m.id = mesh_id
+        m.translate, m.scale = tr, float(sc.value)
+        m.n_vertices, m.n_triangles = nv.value, nt.value
+        m.vertices = m.triangles = None  # held by the library
+        return m
+
     def close(self):
         if getattr(self, "id", None) is not None:
             self.L.ariel_mesh_destroy(self.id)

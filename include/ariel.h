@@ -291,6 +291,35 @@ ariel_status ariel_selftest_barrier_timeout(double timeout_ms);
 ariel_status ariel_mesh_create(const float* vertices, int32_t n_vertices, const int32_t* triangles,
                                int32_t n_triangles, const float* translate, float scale, int32_t* mesh_id);
 ariel_status ariel_mesh_destroy(int32_t mesh_id);
+/* A registered mesh's vertex and triangle counts and placement (any pointer may be null). */
+ariel_status ariel_mesh_info(int32_t mesh_id, int32_t* n_vertices, int32_t* n_triangles, float* translate,
+                             float* scale);
+
+/* Scene files (SceneLoader, src/scene/sceneloader.cpp:11-131, 346-443): the reference's JSON
+ * scene (settings, globalforces, transforms, meshfiles, geoms, sim) into *desc.  A box liquid
+ * becomes an AsimBox, a sphere solid an AsimSphere; box solids and solids read from OBJ files
+ * (paths relative to the scene file, src/geom/obj/obj.cpp) are registered as static meshes
+ * (ariel_mesh_create), listed in desc->mesh, and stay registered until ariel_mesh_destroy.
+ * What the path cannot represent (liquids from meshes, animated meshes, rotations, non-uniform
+ * scaling of spheres or meshes, geometry appearing after frame 0, non-cubic grids, more boxes,
+ * spheres, meshes or forces than the ABI holds, missing ids, unreadable files) returns
+ * ARIEL_ERR_INVALID_ARG with the reason in `error` (when given) and registers nothing.  The
+ * reference seeds liquid particles at lattice-cell centres: pass jitter 0 to match it.
+ * Host-side only (no device needed). */
+typedef struct AsimSceneInfo {
+    int32_t dim;
+    int32_t reserved;
+    double density;           /* settings.density as written (desc->density is its float) */
+    double step_size;
+    char partio_output[512];  /* settings' output paths ("" when absent) */
+    char vdb_output[512];
+    char mesh_output[512];
+} AsimSceneInfo;
+ariel_status ariel_scene_load(const char* path, float jitter, uint64_t seed, AsimSceneDesc* desc,
+                              AsimSceneInfo* info, char* error, int32_t error_len);
+/* The same from the file's text; `base_dir` resolves OBJ paths. */
+ariel_status ariel_scene_parse(const char* json_text, const char* base_dir, float jitter, uint64_t seed,
+                               AsimSceneDesc* desc, AsimSceneInfo* info, char* error, int32_t error_len);
 
 /* Checkpoints: every piece of state a step reads from the previous one (particles, pressure
  * warm start, frame counter, density normaliser) of every scene of the handle, in one file.

@@ -43,6 +43,22 @@ inline void check(ariel_status st, const char* what) {
     if (st != ARIEL_OK) throw Error(st, what);
 }
 
+// A reference scene file (SceneLoader's JSON) read by the library (ariel_scene_load): the scene
+// description, with the settings' grid size, density, step size and output paths in *info when
+// given.  Box and OBJ solids are registered meshes listed in the description; release them with
+// ariel_mesh_destroy once no handle is to be created from it.  Throws Error with the loader's
+// reason for what the path cannot represent.
+inline AsimSceneDesc LoadScene(const std::string& path, AsimSceneInfo* info = nullptr, float jitter = 0.0f,
+                               uint64_t seed = 1) {
+    AsimSceneDesc d;
+    AsimSceneInfo in;
+    char why[512];
+    const ariel_status st = ariel_scene_load(path.c_str(), jitter, seed, &d, &in, why, (int32_t)sizeof why);
+    if (st != ARIEL_OK) throw Error(st, std::string("LoadScene(") + path + "): " + why);
+    if (info) *info = in;
+    return d;
+}
+
 // Host copy of the particle state, id order, xyz-interleaved vectors.
 struct Particles {
     std::vector<float> pos, vel, density, mass;

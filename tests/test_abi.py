@@ -62,9 +62,10 @@ def test_struct_layouts_match_the_header(tmp_path):
     import shutil
     import subprocess
     structs = ["AsimBox", "AsimSphere", "AsimSceneDesc", "AsimParams", "AsimStats", "AsimSolverTotals",
-               "AsimServerConfig", "AsimRequestInfo", "AsimServerStats"]
+               "AsimServerConfig", "AsimRequestInfo", "AsimServerStats", "AsimSceneInfo"]
     fields = [("AsimSceneDesc", "seed"), ("AsimSceneDesc", "n_mesh"), ("AsimSceneDesc", "mesh"),
-              ("AsimParams", "sweep_brick"), ("AsimStats", "stage_ms")]
+              ("AsimParams", "sweep_brick"), ("AsimParams", "reseed_max"), ("AsimStats", "stage_ms"),
+              ("AsimSceneInfo", "mesh_output")]
     src = tmp_path / "sizes.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ariel.h"', "int main(void) {"]
     lines += ['printf("%s %%zu\\n", sizeof(%s));' % (s, s) for s in structs]

@@ -118,6 +118,76 @@ def test_scene_file_mesh_solids(tmp_path):
     assert state_bytes([d], prm) > state_bytes([base], prm)  # the meshes' trees and their solids
 
 
+def test_native_loader_reads_json_as_the_reference_files_write_it(tmp_path):
+    """The library's own JSON reader: escapes in ids and paths, exponents, a repeated key (the
+    last value counts, as Python's json keeps it), numbers given as strings, and the same scene
+    whether read from the file or from its text."""
+    from ariel_b200.sceneloader import scene_from_json
+    text = json.dumps(_scene_json(64)).replace('"tank"', '"t\\u00e4nk"')  # an escaped id, used twice
+    text = text.replace('"step_size": 0.0020833333333333333', '"step_size": 2.0833333333333333e-3, "step_size": "0.0020833333333333333"')
+    p = tmp_path / "escaped.json"
+    p.write_text(text)
+    d, info = load_scene(str(p))
+    ref, _ = scene_from_json(_scene_json(64))
+    assert bytes(d) == bytes(ref)
+    assert info["step_size"] == 1.0 / 480.0
+    d2, _ = scene_from_json(json.loads(text))
+    assert bytes(d2) == bytes(d)
+
+
+@pytest.mark.parametrize("bad", ["json", "unknown_mesh", "unknown_geom", "too_many_meshes", "missing_file"])
+def test_native_loader_refusals(tmp_path, bad):
+    from ariel_b200.sceneloader import scene_from_json
+    root = _scene_json(64)
+    if bad == "unknown_mesh":
+        root["geoms"][0]["geom_frames"] = ["nothing"]
+    elif bad == "unknown_geom":
+        root["sim"][0]["geom"] = "nothing"
+    elif bad == "too_many_meshes":
+        for k in range(A.MAX_MESHES + 1):
+            root["meshfiles"].append({"id": "b%d" % k, "mesh_gen": "box", "point0": {"x": k, "y": 0, "z": 0},
+                                      "point1": {"x": k + 1, "y": 1, "z": 1}})
+            root["geoms"].append({"id": "g%d" % k, "type": "mesh", "geom_frames": ["b%d" % k],
+                                  "transform_frames": ["identity"]})
+            root["sim"].append({"geom": "g%d" % k, "type": "solid"})
+    elif bad == "missing_file":
+        root["meshfiles"].append({"id": "gone", "file": "gone.obj"})
+    if bad == "json":
+        p = tmp_path / "broken.json"
+        p.write_text(json.dumps(root)[:-3])
+        with pytest.raises(SceneError, match="JSON"):
+            load_scene(str(p))
+    else:
+        with pytest.raises(SceneError):
+            scene_from_json(root, base_dir=str(tmp_path))
+    with pytest.raises(SceneError, match="cannot read"):
+        load_scene(str(tmp_path / "no_such_scene.json"))
+
+
+def test_cpp_host_loads_a_scene_file(tmp_path):
+    """ariel::LoadScene from a C++ program (tests/cpp/scene_load_main.cpp), no GPU needed: the
+    same description as the Python loader, mesh solids registered, and a refusal's reason."""
+    import subprocess
+    from test_cpp_wrapper import _build
+    (tmp_path / "rock.obj").write_text(_CUBE_OBJ)
+    root = _scene_json(64)
+    root["meshfiles"].append({"id": "rockfile", "file": "rock.obj"})
+    root["transforms"].append({"id": "placed", "translation": {"x": 44, "y": 10, "z": 40},
+                               "scale": {"x": 6, "y": 6, "z": 6}})
+    root["geoms"].append({"id": "r2", "type": "mesh", "geom_frames": ["rockfile"], "transform_frames": ["placed"]})
+    root["sim"].append({"geom": "r2", "type": "solid"})
+    good, bad = tmp_path / "scene.json", tmp_path / "rotated.json"
+    good.write_text(json.dumps(root))
+    bad.write_text(json.dumps(_scene_json(64, rotation={"x": 0, "y": 30, "z": 0})))
+    r = subprocess.run([_build(tmp_path, "scene_load_main"), str(good), str(bad)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "dim 64 density 0.500 step 0.002083 partio out/particles.geo" in r.stdout
+    assert ("liquids 1 box 0.400 0.600 1.000 solids 1 sphere 0.6000 0.3000 0.5000 r 0.1500 meshes 1 forces 1"
+            in r.stdout), r.stdout
+    assert "mesh 0 vertices 8 triangles 12 scale 0.093750" in r.stdout
+    assert "refused: LoadScene(" in r.stdout and "rotated geometry" in r.stdout
+
+
 @pytest.mark.gpu
 def test_checkpoint_continues_bit_identically(tmp_path):
     descs = [dambreak(16, seed=1), dambreak(20, seed=3, spheres=[((0.6, 0.3, 0.5), 0.15)])]
