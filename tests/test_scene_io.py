@@ -164,6 +164,23 @@ def test_native_loader_refusals(tmp_path, bad):
         load_scene(str(tmp_path / "no_such_scene.json"))
 
 
+def test_native_loader_error_buffer(tmp_path):
+    """The reason is cut to the caller's buffer (NUL-terminated), and no buffer is needed."""
+    import ctypes as C
+    from ariel_b200 import _lib
+    L = _lib.lib()
+    d, info = A.AsimSceneDesc(), A.AsimSceneInfo()
+    text = json.dumps(_scene_json(64, rotation={"x": 0, "y": 30, "z": 0})).encode()
+    buf = C.create_string_buffer(b"#" * 16, 16)
+    assert L.ariel_scene_parse(text, b".", 0.0, 1, C.byref(d), C.byref(info), buf, 8) == A.ARIEL_ERR_INVALID_ARG
+    assert buf.raw[:8] == b"rotated\0" and buf.raw[8:] == b"#" * 8
+    assert L.ariel_scene_parse(text, b".", 0.0, 1, C.byref(d), None, None, 0) == A.ARIEL_ERR_INVALID_ARG
+    assert L.ariel_scene_parse(None, b".", 0.0, 1, C.byref(d), None, None, 0) == A.ARIEL_ERR_INVALID_ARG
+    ok = json.dumps(_scene_json(64)).encode()
+    assert L.ariel_scene_parse(ok, None, 0.0, 1, C.byref(d), None, None, 0) == A.ARIEL_OK
+    assert d.dim == 64 and d.n_liquid == 1
+
+
 def test_cpp_host_loads_a_scene_file(tmp_path):
     """ariel::LoadScene from a C++ program (tests/cpp/scene_load_main.cpp), no GPU needed: the
     same description as the Python loader, mesh solids registered, and a refusal's reason."""
