@@ -300,7 +300,7 @@ double num(const JVal& v, const char* what) {
 
 long long integer(const JVal& v, const char* what) {
     if (v.kind == JVal::Num) {
-        if (!std::isfinite(v.num)) fail(std::string(what) + " is not a finite number");
+        if (!(std::fabs(v.num) < 9.0e18)) fail(std::string(what) + " is out of range");
         return (long long)std::trunc(v.num);
     }
     if (v.kind == JVal::Bool) return v.b ? 1 : 0;
